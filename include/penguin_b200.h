@@ -1,0 +1,217 @@
+/*
+ * penguin_b200.h -- C ABI of the B200-native PEnGUIn hydro step.
+ *
+ * One disk run ("pg_run") owns its grid on one GPU: the conserved-variable
+ * planes (Sigma, v_r, v_phi) in FP64, stored ring-major in *physical* azimuth
+ * order, plus per-ring FARGO bookkeeping (rot_j, inc_j, rot_v, res_v) and the
+ * six fixed ghost rings on each radial edge.  Every entry point returns an
+ * int status (PG_OK == 0); the text of the last failure is available from
+ * pg_last_error().  Nothing here calls exit() or traps on the device.
+ *
+ * The reference binds these paths as mangled C++ symbols called only from
+ * main.cu kernel(); each declaration below names the reference interface it
+ * replaces (file:line within fungjeff/penguin_2_0).
+ */
+#ifndef PENGUIN_B200_H
+#define PENGUIN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PG_OK                 0
+#define PG_ERR_CUDA           1   /* a CUDA runtime call failed                 */
+#define PG_ERR_PARAMS         2   /* unsupported or inconsistent parameters     */
+#define PG_ERR_NONFINITE      3   /* NaN/Inf or non-positive density detected   */
+#define PG_ERR_DT_COLLAPSE    4   /* dt/endtime < 1e-12 (timestep.cu:143)       */
+#define PG_ERR_TIMEOUT        5   /* a bounded device wait gave up              */
+#define PG_ERR_IO             6   /* dump file missing / short / wrong size     */
+#define PG_ERR_STATE          7   /* dump violates an invariant the run keeps   */
+#define PG_ERR_NOMEM          8   /* device allocation failed                   */
+#define PG_ERR_ARG            9   /* NULL pointer or bad size                   */
+
+/* ---- parameters ---------------------------------------------------------
+ * Field names are those of include/variable_types.h:11-20 and
+ * include/global.h:16-96 of the reference, turned from compile-time
+ * constants into runtime values.  n_pad (6) and arrsize (128, so 116 interior
+ * cells per pencil chunk) are fixed: the sweep results depend on that chunk
+ * size (the viscosity stencil at chunk edges sees un-remapped neighbours).   */
+typedef struct pg_params {
+  /* grid (variable_types.h:11-20) */
+  int    ndim;            /* 2 (r-phi) or 3 (r-phi-theta)                      */
+  int    imax, jmax, kmax;
+  /* physics switches (global.h:16-26); flat_flag 1 == "#define flat_flag"   */
+  int    flat_flag, bary_flag, EOS, plnt_flag, FrRot_flag, kill_flag;
+  int    visc_flag, FARGO_flag, dump_flag;
+  /* disk (global.h:32-37) */
+  double p_alpha, p_beta, ss_alpha, sc_h, Sigma_0;
+  /* planet (global.h:43-46) */
+  double M_p, R_p, t_growth, rs_fac;
+  /* hydro (global.h:52-69) */
+  double gam, courant;
+  int    nlft, nrgh, nudr, ntop;
+  double endtime, tmovie;
+  int    ncycend, nprin;
+  /* grid (global.h:76-96) */
+  double xmin, xmax, ymin, ymax, zmin, zmax;
+  int    ngeomx, ngeomy, ngeomz;
+  int    grspx, grspy, grspz;
+  double dx_min, dx_max, dy_min, dy_max, dz_min, dz_max;  /* grid.cu lg 4-6 */
+  /* run extras that the reference hard-codes elsewhere or lacks */
+  uint64_t seed;          /* splitmix64 seed of the initial-condition noise   */
+  double noise_amp;       /* multiplicative Sigma noise amplitude (1e-4)      */
+  double kill_rin;        /* wave damping for r < kill_rin (0 = none)         */
+  double kill_rout;       /* wave damping for r > kill_rout (0 = none)        */
+  int    precision;       /* 0 = FP64 throughout                              */
+  int    reserved[7];
+} pg_params;
+
+/* Planet state, same fields and order as struct body (variable_types.h:26-37). */
+typedef struct pg_body {
+  double m, x, y, vx, vy, fx, fy, rs;
+} pg_body;
+
+/* Per-step scalars of the fused device-resident loop (main.cu:343-441). */
+typedef struct pg_clock {
+  double simtime;   /* main.cu:272                                          */
+  double timem;     /* time since last dump, main.cu:273                    */
+  double dt;        /* dt carried into the next get_dt (old_dt restored)    */
+  double dt_used;   /* dt of the last step actually taken                   */
+  double frrot;     /* frame rotation FrRot                                 */
+  int64_t ncycle;   /* steps taken                                          */
+  int    make_pict; /* last step landed on tmovie or endtime                */
+  int    done;      /* endtime reached                                      */
+  int    status;    /* device status word (PG_OK or PG_ERR_*)               */
+  int    pad;
+} pg_clock;
+
+typedef struct pg_run pg_run;
+
+/* ---- parameters / host-side set-up -------------------------------------- */
+
+/* Fills *p with the reference defaults of include/global.h:16-96 and
+ * include/variable_types.h:11-20 (imax=850, jmax=2000, kmax=1, ...).       */
+int pg_default_params(pg_params *p);
+
+/* Fills *p with a named workload: 0 = 2D 256x768 FP64 disk, 1 = 3D
+ * 128x1024x32 spherical disk, 2 = 2D 1024x3072 disk.                       */
+int pg_config_params(int which, pg_params *p);
+
+/* Checks a parameter set; PG_ERR_PARAMS with a message for combinations the
+ * reference does not implement (EOS != 0, bary_flag, ...) or whose sweep
+ * chunking would read already-updated cells (jmax % 116 in 1..5).          */
+int pg_check_params(const pg_params *p);
+
+/* Size in bytes of one hydr_ring record of the dump layout
+ * (variable_types.h:67-97): 72*jmax + 96.                                  */
+size_t pg_ring_bytes(int jmax);
+
+/* Writes the seeded initial condition as a reference-layout dump
+ * (binary/binary_<label>_00000, main.cu:124 + output.cu:48-55).  Replaces
+ * init_grid/init_den/init_speed/init_cells (init.cpp:3-249) with the noise
+ * described by p->seed / p->noise_amp.                                    */
+int pg_write_ic(const pg_params *p, const char *path);
+int pg_build_ic(const pg_params *p, void *rings, size_t bytes);
+
+/* Run label of create_label() (output.cu:57-88) into buf.                  */
+int pg_label(const pg_params *p, char *buf, size_t len);
+
+/* ---- run lifetime -------------------------------------------------------- */
+
+/* Replaces the allocation block of main.cu:141-219.  Device memory is owned
+ * by the run; the caller owns only the host buffers passed in.            */
+int pg_create(const pg_params *p, int device, pg_run **out);
+int pg_destroy(pg_run *run);
+const char *pg_last_error(const pg_run *run);
+int pg_sync(pg_run *run);
+
+/* Restart path: copy_bfile + copy_grid + init_den/init_speed + init_bound
+ * (main.cu:246-284, init.cpp:59-90, 253-413).  rings holds imax*kmax records
+ * in the dump layout.                                                      */
+int pg_load_rings(pg_run *run, const void *rings, size_t bytes);
+int pg_load_dump(pg_run *run, const char *path);
+/* save_cells (output.cu:48-55) after a device->host copy (main.cu:400).    */
+int pg_save_rings(pg_run *run, void *rings, size_t bytes);
+int pg_save_dump(pg_run *run, const char *path);
+
+/* ---- the reference's step entry points ----------------------------------- */
+
+/* get_dt (timestep.cu:112-149): CFL rate max over the grid, then
+ * min(1.1*dt_old, courant/max).                                           */
+int pg_get_dt(pg_run *run, double dt_old, double frrot, double *dt_out);
+
+/* Index_Shift (orbital_advection.cu:45-69): per-ring inc_j, res_v, rot_v.  */
+int pg_index_shift(pg_run *run, double dt, double frrot);
+
+/* bundle_sweep2D (ppm.cu:358-386): radial sweep, azimuthal sweep with the
+ * FARGO integer shift applied at its store, rotate_rings.                 */
+int pg_sweep2d(pg_run *run, double dt, const pg_body *planet, double frrot);
+
+/* The 3D counterpart the reference calls at main.cu:376 but never defines:
+ * radial, azimuthal and polar sweeps, then rotate_rings.                  */
+int pg_sweep3d(pg_run *run, double dt, const pg_body *planet, double frrot);
+
+/* Wave damping toward the initial axisymmetric profile for r < kill_rin and
+ * r > kill_rout.  The live reference has no damping (global.h:22); this
+ * restates the dead kill_wave.cu:19-40 formula on the current layout.      */
+int pg_damp(pg_run *run, double dt);
+
+/* GPU_output_reduction (device_func.cu:169-198): mode 0 disk mass,
+ * 8 radial force, 9 torque; same per-ring 1024-wide tree order.            */
+int pg_reduce(pg_run *run, const pg_body *planet, double exclude, int mode,
+              double *out);
+
+/* ---- planet (planet.cu:11-93), host arithmetic --------------------------- */
+int pg_init_planet(const pg_params *p, pg_body *planet, double *frrot);
+double pg_set_M_p(const pg_params *p, double t);
+int pg_planet_forces(pg_run *run, pg_body *planet, double frrot, double simtime);
+int pg_kick_drift_kick(const pg_params *p, pg_body *planet, double *frrot,
+                       double dt, int kick);
+double pg_get_ecc(const pg_body *planet, double frrot);
+double pg_get_E(const pg_body *planet, double frrot);
+
+/* ---- fused device-resident loop ------------------------------------------ */
+
+/* Resets the run clock as main.cu:270-330 does for a restart from frame
+ * startat: simtime = tmovie*startat, dt = endtime, planet from init_planet. */
+int pg_clock_reset(pg_run *run, int startat);
+int pg_clock_get(pg_run *run, pg_clock *clk, pg_body *planet);
+
+/* Advances nsteps steps of main.cu:343-441 with dt, FARGO shift, planet
+ * kick-drift-kick and the dt clipping to tmovie/endtime all on the device:
+ * no host synchronisation inside.  Stops early (without error) after a
+ * step that lands on tmovie or endtime, so the caller can dump.  Torque
+ * and mass every nprin steps go to a device history read by
+ * pg_history().  *taken gets the number of steps done.                    */
+int pg_advance(pg_run *run, int nsteps, int *taken);
+
+/* Copies up to max rows of the diagnostics history (simtime, mass, torque
+ * normalised as main.cu:421, planet x, y, vx, vy, fx, fy, ecc, a) recorded
+ * since the last call; *rows gets the count.                               */
+int pg_history(pg_run *run, double *rows, int max, int *rows_out);
+
+/* Same as pg_advance but with the step sequence captured once in a CUDA
+ * graph of `chunk` steps and replayed (launch-bound small grids).          */
+int pg_advance_graph(pg_run *run, int nsteps, int chunk, int *taken);
+
+/* ---- device buffers (for harnesses that keep data resident) -------------- */
+typedef struct pg_device_view {
+  double *sigma, *vr, *vphi;  /* current planes, [imax*kmax][jmax] physical  */
+  int64_t row_stride;         /* elements between rings                      */
+  int    imax, jmax, kmax;
+  int    pad;
+  void  *stream;              /* cudaStream_t the run launches on            */
+} pg_device_view;
+int pg_device_view_get(pg_run *run, pg_device_view *view);
+
+/* Count of kernel launches issued by this run since creation.             */
+int64_t pg_launch_count(const pg_run *run);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PENGUIN_B200_H */

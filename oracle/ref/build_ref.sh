@@ -1,0 +1,28 @@
+#!/bin/bash
+# Build the reference's own CUDA hydro step for one workload (oracle/_ref).
+#   oracle/ref/build_ref.sh <name> <params.json>
+# Compiles the reference's translation units where they lie (read-only tree,
+# default /root/reference, override with PG_REFERENCE) against per-workload
+# copies of its two configuration headers (gen_headers.py) and links them
+# with ref_harness.cu.  Output: oracle/_ref/<name>/penguin_ref (git-ignored).
+set -euo pipefail
+NAME=$1
+PJSON=$2
+REF=${PG_REFERENCE:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT=$HERE/../_ref/$NAME
+mkdir -p "$OUT/obj"
+python3 "$HERE/gen_headers.py" "$PJSON" "$OUT" "$REF" > /dev/null
+NVCC="nvcc -O3 -gencode arch=compute_100a,code=sm_100a -lineinfo -w"
+INC="-I$OUT/include -I$REF/include"
+pids=()
+for src in shared/variable_types shared/global disk_profile/disk_profile output/output \
+           timestep/timestep ppm/ppm planet/planet orbital_advection/orbital_advection; do
+  $NVCC --device-c -o "$OUT/obj/$(basename $src).o" "$REF/src/$src.cu" $INC &
+  pids+=($!)
+done
+$NVCC --device-c -o "$OUT/obj/harness.o" "$HERE/ref_harness.cu" $INC -I"$REF" &
+pids+=($!)
+for p in "${pids[@]}"; do wait "$p"; done
+$NVCC -o "$OUT/penguin_ref" "$OUT"/obj/*.o
+echo "$OUT/penguin_ref"

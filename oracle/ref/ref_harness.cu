@@ -1,0 +1,213 @@
+// ref_harness.cu -- driver that runs the reference's own CUDA hydro step
+// (TEST INFRASTRUCTURE: produces golden vectors, never part of the product).
+//
+// It is linked with the reference's unmodified translation units
+// (src/shared, src/disk_profile, src/output, src/timestep, src/ppm,
+// src/planet, src/orbital_advection) compiled against per-workload copies of
+// the two configuration headers, and it includes the reference's init.cpp
+// the way main.cu does.  In place of main.cu:kernel() it follows the restart
+// path (main.cu:246-330) from a seeded dump and then the time loop of
+// main.cu:343-441, with these harness changes:
+//   * the ghost rings lft/rgh are allocated zeroed, so their res_v/inc_j
+//     are 0 (the reference relies on fresh heap pages for that);
+//   * after bundle_sweep2D a wave-damping kernel acts on cells with
+//     r < h_kill_rin or r > h_kill_rout (the workload's damping zones);
+//   * after every step it records simtime, dt, mass (mode 0) and torque
+//     (mode 9, normalised as main.cu:421) and, after the listed steps, the
+//     full rings in the dump layout.
+//
+// usage: penguin_ref <ic_dump> <nsteps> <outdir> <steps-to-save, comma separated>
+#include <unistd.h>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <math.h>
+
+#include "variable_types.h"
+#include "global.h"
+#include "disk_profile.h"
+#include "ppm.h"
+#include "output.h"
+#include "timestep.h"
+#include "planet.h"
+#include "orbital_advection.h"
+#include "cuSafe.cu"
+#include "harness_params.h"
+
+using namespace std;
+
+sdp *zxa, *zxc, *zdx, *zya, *zyc, *zdy, *zza, *zzc, *zdz;
+
+#include "init.cpp"
+
+// Damping toward the axisymmetric profile val[] (the rule used by the
+// oracle and by the CUDA path): f = dt r^-1.5 (distance into zone / width).
+__global__ void harness_damp(hydr_ring *rings, SymDisk *val, sdp dt, int nring)
+{
+  int n = blockIdx.x;
+  if (n >= nring) return;
+  sdp r = rings[n].xc, f;
+  if (h_kill_rin > 0.0 && r < h_kill_rin) f = (h_kill_rin - r) / (h_kill_rin - xmin);
+  else if (h_kill_rout > 0.0 && r > h_kill_rout) f = (r - h_kill_rout) / (xmax - h_kill_rout);
+  else return;
+  f *= dt * pow(r, -1.5);
+  int idx = rings[n].i + imax * rings[n].k;
+  sdp rad_cyl = r;
+  if (ngeomz == 5) rad_cyl *= sin(rings[n].zc);
+  sdp cs2 = get_cs2(rad_cyl);
+  for (int j = threadIdx.x; j < jmax; j += blockDim.x) {
+    rings[n].r[j] += f * (val[idx].r - rings[n].r[j]);
+    rings[n].u[j] += f * (val[idx].u - rings[n].u[j]);
+    rings[n].v[j] += f * (val[idx].v - rings[n].v[j]);
+    rings[n].w[j] += f * (-rings[n].w[j]);
+    rings[n].p[j] = rings[n].r[j] * cs2;
+  }
+}
+
+int main(int argc, char **argv)
+{
+  if (argc < 5) {
+    fprintf(stderr, "usage: %s <ic_dump> <nsteps> <outdir> <s1,s2,...>\n", argv[0]);
+    return 2;
+  }
+  const char *icpath = argv[1];
+  int nsteps = atoi(argv[2]);
+  string outdir = argv[3];
+  bool keep[100000] = {false};
+  {
+    string ks = argv[4];
+    stringstream ss(ks);
+    string tok;
+    while (getline(ss, tok, ',')) {
+      int v = atoi(tok.c_str());
+      if (v > 0 && v < 100000) keep[v] = true;
+    }
+  }
+
+  GPU_plan *set = new GPU_plan[1];
+  set[0].id = 0;
+  set[0].N_ring = imax * kmax;
+  CudaSafeCall(cudaSetDevice(0));
+  CudaSafeCall(cudaDeviceSetCacheConfig(cudaFuncCachePreferShared));
+  CudaSafeCall(cudaStreamCreate(&set[0].stream));
+  CudaSafeCall(cudaEventCreate(&set[0].event));
+  set[0].memsize = set[0].N_ring * sizeof(hydr_ring);
+  set[0].istart = 0;
+  set[0].iblk = set[0].N_ring / kmax;
+  set[0].kstart = 0;
+  set[0].kblk = kmax;
+  set[0].sx_grid = dim3(jmax, set[0].kblk, 1);
+  set[0].sy_grid = dim3(set[0].iblk, set[0].kblk, 1);
+  set[0].sz_grid = dim3(set[0].iblk, jmax, (set[0].kblk / realarr) + (bool)(set[0].kblk % realarr));
+  set[0].t_grid = dim3(set[0].iblk, set[0].kblk, 1);
+  CudaSafeCall(cudaMalloc((void **)&set[0].rings, set[0].memsize));
+  CudaSafeCall(cudaMallocHost((void **)&set[0].h_rings, set[0].memsize));
+  CudaSafeCall(cudaMalloc((void **)&set[0].lft, n_pad * kmax * sizeof(hydr_ring)));
+  CudaSafeCall(cudaMalloc((void **)&set[0].rgh, n_pad * kmax * sizeof(hydr_ring)));
+  CudaSafeCall(cudaMalloc((void **)&set[0].val, imax * kmax * sizeof(SymDisk)));
+  CudaSafeCall(cudaMalloc((void **)&set[0].dt, sizeof(sdp)));
+  CudaSafeCall(cudaMallocHost((void **)&set[0].h_dt, sizeof(sdp)));
+  CudaSafeCall(cudaMallocHost((void **)&set[0].dt_1D, sizeof(sdp) * set[0].iblk));
+  CudaSafeCall(cudaMallocHost((void **)&set[0].dt_2D, sizeof(sdp) * set[0].iblk * set[0].iblk));
+  CudaSafeCall(cudaMalloc((void **)&set[0].d_output, sizeof(sdp)));
+  CudaSafeCall(cudaMallocHost((void **)&set[0].h_output, sizeof(sdp)));
+
+  hydr_ring *lft = (hydr_ring *)calloc(n_pad * kmax, sizeof(hydr_ring));
+  hydr_ring *rgh = (hydr_ring *)calloc(n_pad * kmax, sizeof(hydr_ring));
+  hydr_ring *udr = (hydr_ring *)calloc(n_pad * imax, sizeof(hydr_ring));
+  hydr_ring *top = (hydr_ring *)calloc(n_pad * imax, sizeof(hydr_ring));
+  SymDisk *val = new SymDisk[imax * kmax];
+  zxa = new sdp[imax]; zxc = new sdp[imax]; zdx = new sdp[imax];
+  zya = new sdp[jmax]; zyc = new sdp[jmax]; zdy = new sdp[jmax];
+  zza = new sdp[kmax]; zzc = new sdp[kmax]; zdz = new sdp[kmax];
+
+  // restart path main.cu:246-262
+  ifstream sfile(icpath, ios::in | ios::binary);
+  if (!sfile) { fprintf(stderr, "cannot open %s\n", icpath); return 3; }
+  sfile.read((char *)set[0].h_rings, set[0].memsize);
+  if (!sfile) { fprintf(stderr, "short read of %s\n", icpath); return 3; }
+  copy_grid(set);
+
+  sdp dt = endtime;
+  sdp simtime = 0.0;
+  sdp timem = 0.0;
+  int ncycle = 0, ncycp = 0;
+  init_den(val);
+  init_speed(val);
+  init_bound(lft, rgh, udr, top);
+  CudaSafeCall(cudaMemcpy(set[0].rings, set[0].h_rings, set[0].memsize, cudaMemcpyHostToDevice));
+  CudaSafeCall(cudaMemcpy(set[0].lft, lft, n_pad * kmax * sizeof(hydr_ring), cudaMemcpyHostToDevice));
+  CudaSafeCall(cudaMemcpy(set[0].rgh, rgh, n_pad * kmax * sizeof(hydr_ring), cudaMemcpyHostToDevice));
+  CudaSafeCall(cudaMemcpy(set[0].val, val, imax * kmax * sizeof(SymDisk), cudaMemcpyHostToDevice));
+  CudaSafeCall(cudaDeviceSynchronize());
+
+  body planet;
+  sdp FrRot;
+  init_planet(planet, FrRot);
+  planet_forces(planet, FrRot, set, simtime);
+
+  string hname = outdir + "/hist.txt";
+  FILE *hf = fopen(hname.c_str(), "w");
+  if (!hf) { fprintf(stderr, "cannot write %s\n", hname.c_str()); return 4; }
+  bool make_pict = false, cont_simu = true;
+  sdp old_dt = 0.0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0); cudaEventCreate(&e1);
+  float sweep_ms = 0.f;
+  for (int s = 0; s < nsteps && cont_simu; s++) {
+    dt = get_dt(dt, set, FrRot);
+    if (ncycle == ncycend) cont_simu = false;
+    if (simtime + dt >= endtime) { old_dt = dt; dt = endtime - simtime; make_pict = true; cont_simu = false; }
+    if (timem + dt >= tmovie) { old_dt = dt; dt = tmovie - timem; make_pict = true; }
+    sdp dt_used = dt;
+    Index_Shift(set, dt, FrRot);
+    #if plnt_flag > 0
+    kick_drift_kick(planet, FrRot, set, simtime, 0.5 * dt, true);
+    #endif
+    cudaEventRecord(e0, set[0].stream);
+    bundle_sweep2D(set, dt, planet, FrRot);
+    cudaEventRecord(e1, set[0].stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    sweep_ms += ms;
+    if (h_kill_rin > 0.0 || h_kill_rout > 0.0) {
+      harness_damp<<<imax * kmax, 256, 0, set[0].stream>>>(set[0].rings, set[0].val, dt, imax * kmax);
+      CudaCheckError();
+      CudaSafeCall(cudaStreamSynchronize(set[0].stream));
+    }
+    simtime += dt; timem += dt; ncycle++; ncycp++;
+    #if plnt_flag > 0
+    kick_drift_kick(planet, FrRot, set, simtime, dt, false);
+    planet_forces(planet, FrRot, set, simtime);
+    kick_drift_kick(planet, FrRot, set, simtime, 0.5 * dt, true);
+    #endif
+    if (make_pict) { timem = 0.0; make_pict = false; dt = old_dt; }
+    sdp mass = GPU_output_reduction(set, planet, 0.0);
+    sdp torque = 0.0;
+    #if plnt_flag > 0
+    torque = GPU_output_reduction(set, planet, 0.0, 9) / (M_p * M_p * pow(R_p, 1.0 - p_alpha + (p_beta - 1.0)) / (sc_h * sc_h));
+    #endif
+    fprintf(hf, "%d %a %a %a %a %a %a\n", s, simtime, dt_used, mass, torque, FrRot, planet.y);
+    if (s + 1 < 100000 && keep[s + 1]) {
+      CudaSafeCall(cudaMemcpy(set[0].h_rings, set[0].rings, set[0].memsize, cudaMemcpyDeviceToHost));
+      char nm[64];
+      snprintf(nm, sizeof nm, "/state_%05d.bin", s + 1);
+      ofstream of((outdir + nm).c_str(), ios::out | ios::binary);
+      save_cells(of, set);
+      of.close();
+    }
+  }
+  fclose(hf);
+  printf("{\"steps\": %d, \"cells\": %d, \"sweep_ms_total\": %.6f}\n", ncycle, imax * jmax * kmax, sweep_ms);
+  CudaSafeCall(cudaFree(set[0].rings));
+  CudaSafeCall(cudaFreeHost(set[0].h_rings));
+  CudaSafeCall(cudaFree(set[0].lft));
+  CudaSafeCall(cudaFree(set[0].rgh));
+  CudaSafeCall(cudaFree(set[0].val));
+  return 0;
+}

@@ -1,0 +1,300 @@
+// pg_chunk.cuh -- the ppmlr chain (ppmlr.cu:2-56) for one 128-cell chunk,
+// specialised per sweep axis at compile time.
+//   AXIS 0: radial (cylindrical R, ngeomx 1, or spherical r, ngeomx 2)
+//   AXIS 1: azimuthal (ngeomy 3 cylindrical / 4 spherical)
+//   AXIS 2: polar angle (ngeomz 5)
+// SPH selects the spherical geometry branches (3D), THREED keeps the w
+// component alive.
+#pragma once
+#include "pg_ppm.cuh"
+
+namespace pgd {
+
+// Per-thread inputs of one chunk cell.
+struct CellIn {
+  double rad;    // ppmlr's rad argument (ring radius; r sin(theta) in sweepy)
+  double azi;    // cell-centre azimuth in the physical frame
+  double pol;    // polar angle (0 in 2D)
+  double vrot;   // res_v / rad_cyl of the cell's ring
+  double dvol0;  // Eulerian cell volume along the sweep
+};
+
+template <int AXIS, bool SPH>
+__device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, const ChunkShm &S,
+                                           const Body &pl, const Phys &ph, double &ftot) {
+  if (AXIS == 0) {
+    // get_fx_bound forces.cu:185-224 at the left face xa0[n]
+    double rad = S.xa0[n];
+    double azi = c.azi + hdt * c.vrot;
+    double grav;
+    if (!SPH) {
+      if (ph.plnt) { grav = grav_rad_cyl(rad, azi, c.pol, pl, hdt); grav += -1.0 / rad / rad; }
+      else { double dis = sqrt(rad * rad + c.pol * c.pol); grav = -rad / dis / dis / dis; }
+      double f = grav;
+      f += pow(0.5 * (S.v[n] + S.v[n - 1]), 2) / rad / rad / rad;
+      ftot = f;
+    } else {
+      grav = ph.plnt ? grav_rad_sph(rad, azi, c.pol, pl, hdt) : -1.0 / rad / rad;
+      double f = grav;
+      f += pow(0.5 * (S.w[n] + S.w[n - 1]), 2) / rad / rad / rad;
+      f += pow(0.5 * (S.v[n] + S.v[n - 1]), 2) / rad / pow(rad * sin(c.pol), 2);
+      ftot = f;
+    }
+  } else if (AXIS == 1) {
+    // get_fy forces.cu:265-296 at xa0[n] + hdt v_rot
+    double azi = S.xa0[n] + hdt * c.vrot;
+    if (!SPH) ftot = ph.plnt ? grav_azi_cyl(c.rad, azi, c.pol, pl, hdt) : 0.0;
+    else ftot = ph.plnt ? grav_azi_sph(c.rad, azi, c.pol, pl, hdt) : 0.0;
+  } else {
+    // get_fz_bound forces.cu:298-334 (ngeomz 5) at the face angle xa0[n]
+    double pol = S.xa0[n];
+    double azi = c.azi + hdt * c.vrot;
+    double grav = ph.plnt ? grav_pol_sph(c.rad, azi, pol, pl, hdt) : 0.0;
+    double rad_cyl = c.rad * sin(pol);
+    double f = grav;
+    f += (pow(0.5 * (S.w[n] + S.w[n - 1]), 2) * cos(pol)) / rad_cyl / rad_cyl / rad_cyl;
+    ftot = f;
+  }
+}
+
+// get_fx / get_fy / get_fz at a cell centre (forces.cu:226-372)
+template <int AXIS, bool SPH>
+__device__ __forceinline__ double centre_force(int n, double dt, double rad, double azi, double pol,
+                                               const ChunkShm &S, const Body &pl, const Phys &ph) {
+  if (AXIS == 0) {
+    double grav;
+    if (!SPH) {
+      if (ph.plnt) { grav = grav_rad_cyl(rad, azi, pol, pl, dt); grav += -1.0 / rad / rad; }
+      else { double dis = sqrt(rad * rad + pol * pol); grav = -rad / dis / dis / dis; }
+      double f = grav;
+      f += S.v[n] * S.v[n] / rad / rad / rad;
+      return f;
+    } else {
+      grav = ph.plnt ? grav_rad_sph(rad, azi, pol, pl, dt) : -1.0 / rad / rad;
+      double f = grav;
+      f += S.w[n] * S.w[n] / rad / rad / rad;
+      f += S.v[n] * S.v[n] / rad / pow(rad * sin(pol), 2);
+      return f;
+    }
+  } else if (AXIS == 1) {
+    if (!SPH) return ph.plnt ? grav_azi_cyl(rad, azi, pol, pl, dt) : 0.0;
+    return ph.plnt ? grav_azi_sph(rad, azi, pol, pl, dt) : 0.0;
+  } else {
+    double grav = ph.plnt ? grav_pol_sph(rad, azi, pol, pl, dt) : 0.0;
+    double rad_cyl = rad * sin(pol);
+    double f = grav;
+    f += (S.w[n] * S.w[n] * cos(pol)) / rad_cyl / rad_cyl / rad_cyl;
+    return f;
+  }
+}
+
+// The ppmlr chain for one chunk.  All threads of the CTA call it (it has
+// barriers); cells n >= nmax take no part in any phase.  On return r, u, v
+// (and w when THREED) hold the Lagrange-remapped values for 6 <= n < nmax-6.
+template <int AXIS, bool SPH, bool THREED>
+__device__ __forceinline__ void ppm_chunk(ChunkShm &S, int n, int nmax, double dt, double FrRot,
+                                          const CellIn &c, const Body &pl, const Phys &ph) {
+  const bool act = n < nmax;
+  double flat = 0.0;
+  if (act) { S.q[n] = 0.0; S.dx[n] = 0.0; S.umid[n] = 0.0; S.pmid[n] = 0.0; S.tmp1[n] = 0.0; }
+  __syncthreads();
+
+  // ---- flatten flatten.cu:7-40 (steep in tmp1) ----
+  if (ph.flat) {
+    double *steep = S.tmp1;
+    if (act) {
+      bool shock = false;
+      steep[n] = 0.0;
+      if (n >= 2 && n < nmax - 2) {
+        double dp1 = S.p[n + 1] - S.p[n - 1];
+        double dp2 = S.p[n + 2] - S.p[n - 2];
+        if (fabs(dp2) < kSmallp) dp2 = kSmallp;
+        double ddp = fabs(dp1) / fmin(S.p[n + 1], S.p[n - 1]);
+        if (ddp > 0.33) shock = true;
+        if (S.u[n - 1] < S.u[n + 1]) shock = false;
+        if (shock) {
+          ddp = (dp1 / dp2 - 0.75) * 5.0;
+          steep[n] = fmax(0.0, ddp);
+        }
+      }
+    }
+    __syncthreads();
+    if (n >= 2 && n < nmax - 2) flat = fmin(0.5, max3(steep[n - 1], steep[n], steep[n + 1]));
+    __syncthreads();
+  }
+
+  // ---- states states.cu:3-73 ----
+  // al = q, da = dx, a6 = tmp1, cs = umid, csfac = pmid (ppmlr.cu:30-33)
+  const double hdt = 0.5 * dt;
+  Par par;
+  paraset(n, 0, nmax, par, S.dx0, S.q, S.dx, S.tmp1);
+  double ftot = 0.0;
+  if (n >= 2 && n < nmax - 1) face_force<AXIS, SPH>(n, hdt, c, S, pl, ph, ftot);
+  __syncthreads();
+  if (act) {
+    double cs = hdt * sqrt(ph.gam * S.p[n] / S.r[n]) / S.dx0[n];
+    if (AXIS == 1) cs /= c.rad;
+    if (AXIS == 2) cs /= c.rad;
+    S.umid[n] = cs;
+    S.pmid[n] = 1.0 - kFourthd * cs;
+  }
+  double spl = 0.0, spr = 0.0, srl = 0.0, srr = 0.0, sul = 0.0, sur = 0.0;
+  const double *cs = S.umid, *csfac = S.pmid;
+  double *al = S.q, *da = S.dx, *a6 = S.tmp1;
+  parabola(n, 0, nmax, flat, S.p, al, da, a6, par);
+  if (n >= 3 && n < nmax - 2) {
+    double t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
+    spl = fmax(kSmallp, t);
+    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
+    spr = fmax(kSmallp, t);
+  }
+  __syncthreads();
+  parabola(n, 0, nmax, flat, S.r, al, da, a6, par);
+  if (n >= 3 && n < nmax - 2) {
+    double t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
+    srl = fmax(kSmallr, t);
+    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
+    srr = fmax(kSmallr, t);
+  }
+  __syncthreads();
+  parabola(n, 0, nmax, flat, S.u, al, da, a6, par);
+  if (n >= 3 && n < nmax - 2) {
+    double t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
+    sul = t + hdt * ftot;
+    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
+    sur = t + hdt * ftot;
+  }
+  __syncthreads();
+
+  // ---- riemann riemann.cu:76-188, isothermal (119-126) ----
+  if (n >= 3 && n < nmax - 2) {
+    double t1 = 0.5 * (sqrt(spl / srl) + sqrt(spr / srr));
+    double t2 = -0.5 * (sur - sul) / t1;
+    double pm = sqrt(spl * spr) * exp(t2);
+    S.umid[n] = sul - t1 * log(pm / spl);
+    S.pmid[n] = fmax(kSmallp, pm);
+  }
+  __syncthreads();
+
+  // ---- evolve evolve.cu:3-166 (vfac = tmp1) ----
+  double *vfac = S.tmp1;
+  const double xa0n = S.xa0[n < AP ? n : 0];
+  double xa = xa0n, dvol = c.dvol0, dtdm = 0.0, fto1 = 0.0, fto2 = 0.0;
+  if (act) vfac[n] = S.xa0[n] + 0.5 * S.dx0[n];
+  __syncthreads();
+  if (n >= 3 && n < nmax - 2) {
+    double delx;
+    if (AXIS == 0) delx = dt * S.umid[n];
+    else if (AXIS == 1) delx = dt * (S.umid[n] / c.rad - c.vrot - FrRot);
+    else delx = dt * S.umid[n] / c.rad;
+    dtdm = dt / (S.r[n] * c.dvol0);
+    vfac[n] = S.xa0[n] + delx;
+  }
+  __syncthreads();
+  if (n >= 3 && n < nmax - 3) {
+    S.dx[n] = vfac[n + 1] - vfac[n];
+    xa = vfac[n];
+  }
+  __syncthreads();
+  if (n >= 3 && n < nmax - 3) {
+    double xcl = xa + 0.5 * S.dx[n];
+    if (AXIS == 0) {
+      fto1 = centre_force<0, SPH>(n, 0.0, c.rad, c.azi, c.pol, S, pl, ph);
+      fto2 = centre_force<0, SPH>(n, dt, xcl, c.azi + dt * c.vrot, c.pol, S, pl, ph);
+    } else if (AXIS == 1) {
+      fto1 = centre_force<1, SPH>(n, 0.0, c.rad, c.azi, c.pol, S, pl, ph);
+      fto2 = centre_force<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, S, pl, ph);
+    } else {
+      fto1 = centre_force<2, SPH>(n, 0.0, c.rad, c.azi, c.pol, S, pl, ph);
+      fto2 = centre_force<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, S, pl, ph);
+    }
+  }
+  __syncthreads();
+  if (n >= 3 && n < nmax - 2) {
+    double dxn = S.dx[n];
+    if (AXIS == 0) {
+      if (!SPH) { dvol = dxn * (xa + 0.5 * dxn); vfac[n] = 0.5 * (xa + xa0n); }
+      else {
+        dvol = dxn * (xa * (xa + dxn) + dxn * dxn * kThird);
+        vfac[n] = (xa - xa0n) * (kThird * (xa - xa0n) + xa0n) + (xa0n * xa0n);
+      }
+    } else if (AXIS == 1) {
+      dvol = dxn * c.rad; vfac[n] = 1.0;
+    } else {
+      double delx = xa - xa0n;
+      double dum = cos(xa);
+      dvol = (dum - cos(xa + dxn)) * c.rad;
+      if (delx == 0.0) vfac[n] = sin(xa);
+      else vfac[n] = (cos(xa0n) - dum) / delx;
+    }
+  }
+  __syncthreads();
+  if (n >= 3 && n < nmax - 3) {
+    S.r[n] = fmax(S.r[n] * (c.dvol0 / dvol), kSmallr);
+    double dum = S.u[n];
+    double delx = 0.5 * dt * (fto1 + fto2);
+    delx += -dtdm * (S.pmid[n + 1] - S.pmid[n]) * 0.5 * (vfac[n + 1] + vfac[n]);
+    S.u[n] = dum + delx;
+  }
+  __syncthreads();
+
+  // ---- remap remap.cu:14-226: al = tmp1, da = umid, a6 = pmid, flux = dx ----
+  al = S.tmp1; da = S.umid; a6 = S.pmid;
+  paraset(n, 3, nmax - 3, par, S.dx, al, da, a6);
+  double lvol = 0.0;
+  if (AXIS == 0) {
+    if (!SPH) { lvol = xa - xa0n; lvol *= (xa0n + 0.5 * lvol); }
+    else { lvol = xa - xa0n; lvol *= xa0n * xa + kThird * (lvol * lvol); }
+  } else if (AXIS == 1) {
+    lvol = (xa - xa0n) * c.rad;
+  } else {
+    lvol = (cos(xa0n) - cos(xa)) * c.rad;
+  }
+  double dxf = xa - xa0n;
+  const bool delC = (dxf >= 0.0);
+  parabola(n, 3, nmax - 3, flat, S.r, al, da, a6, par);
+  double *flux = S.dx;
+  double dxnn = 0.0, dxnm = 0.0;
+  if (n >= 6 && n < nmax - 5) { dxnn = S.dx[n]; dxnm = S.dx[n - 1]; }
+  __syncthreads();
+  double dxf2 = 0.0, fr = 0.0;
+  if (n >= 6 && n < nmax - 5) {
+    if (delC) {
+      dxf = 0.5 * dxf / dxnm;
+      dxf2 = 1.0 - kFourthd * dxf;
+      fr = (al[n - 1] + da[n - 1] - dxf * (da[n - 1] - dxf2 * a6[n - 1])) * lvol;
+    } else {
+      dxf = 0.5 * dxf / dxnn;
+      dxf2 = 1.0 + kFourthd * dxf;
+      fr = (al[n] - dxf * (da[n] + dxf2 * a6[n])) * lvol;
+    }
+    flux[n] = fr;
+  }
+  __syncthreads();
+  double mm = 0.0, invm = 0.0;
+  if (n >= 6 && n < nmax - 6) {
+    mm = S.r[n] * dvol;
+    double lv = (mm + fr - flux[n + 1]) / c.dvol0;
+    S.r[n] = fmax(kSmallr, lv);
+    invm = 1.0 / (S.r[n] * c.dvol0);
+  }
+  // momentum-like remaps (get_flux remap.cu:1-10)
+  auto remap_field = [&](double *fld) {
+    parabola(n, 3, nmax - 3, flat, fld, al, da, a6, par);
+    if (n >= 6 && n < nmax - 5) {
+      if (delC) flux[n] = (al[n - 1] + da[n - 1] - dxf * (da[n - 1] - dxf2 * a6[n - 1])) * fr;
+      else      flux[n] = (al[n] - dxf * (da[n] + dxf2 * a6[n])) * fr;
+    }
+    __syncthreads();
+    if (n >= 6 && n < nmax - 6) {
+      double fl = flux[n] - flux[n + 1];
+      fld[n] = (fld[n] * mm + fl) * invm;
+    }
+  };
+  remap_field(S.u);
+  remap_field(S.v);
+  if (THREED) remap_field(S.w);
+  __syncthreads();
+}
+
+}  // namespace pgd

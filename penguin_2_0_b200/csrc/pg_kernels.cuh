@@ -1,0 +1,100 @@
+// pg_kernels.cuh -- device-side data of a run and the kernel launchers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pg_ppm.cuh"
+
+namespace pgd {
+
+// Chunking of one pencil direction (ppm.cu:34, 48, 169, 196).
+struct Chunking {
+  int loop;      // number of 116-cell chunks
+  int lim_last;  // lim of the last chunk: n % 116 + 12
+  int stuck;     // n % 116 == 0: the reference never updates the last chunk
+};
+
+__host__ __device__ inline Chunking make_chunking(int n) {
+  Chunking c;
+  c.loop = n / REAL + (n % REAL != 0);
+  c.lim_last = (n % REAL) + 2 * NPAD;
+  c.stuck = (n % REAL == 0);
+  return c;
+}
+
+// Geometry and per-ring tables, all device pointers.  A "row" counts radial
+// rings including the 6 fixed ghost rings on each side (row = i + 6); a
+// "ring" index rk = k*nrg + row.
+struct Tables {
+  int nr, nphi, nk, nrg;
+  Chunking cx, cy, cz;
+  const double *rx, *rdx, *rxvol, *rxc;         // [nrg]
+  const double *radc, *cs2, *nu;                // [nk*nrg]
+  const double *gp;                             // [nk*nrg] ghost-ring pressure
+  const double *y, *dy, *yvol, *yc;             // [nphi]
+  const double *z, *dz, *zvol, *zc;             // [nk + 12]: 6 ghost layers each side
+  const double *val_r, *val_u, *val_v;          // [nk*nrg] damping / FARGO targets
+  const double *damp_g, *damp_pw;               // [nk*nrg] zone factor, r^-1.5
+  const double *tg;                             // [6*nr*4] theta ghost state (udr): r,p,u,v
+  double *res_v, *rot_v;                        // [nk*nrg]
+  int *inc_j, *rot_j;                           // [nk*nrg]
+};
+
+struct Planes {
+  const double *r, *u, *v, *w;
+  double *ro, *uo, *vo, *wo;
+  const double *p0;   // non-null: pressure of a freshly loaded dump (first sweep only)
+};
+
+// The device-resident clock of the fused loop (main.cu:270-441).
+struct DevClock {
+  double simtime, timem, dt, old_dt, dt_step, frrot, frrot_next;
+  double endtime, tmovie, courant;
+  Body planet;
+  long long ncycle, ncycp, ncycend;
+  int make_pict, prin, done, halted, status, pad;
+  unsigned long long cfl_bits;   // max CFL rate as ordered bits (non-negative)
+  int nprin, plnt_flag, frrot_flag, ndim;
+  double M_p, t_growth, rs_fac, sc2, R_p, Sigma_0;
+  double hist_norm;
+  double mass, torque;           // last diagnostics reductions
+  double *hist;                  // device history rows (HIST_COLS each)
+  int hist_count, hist_cap;
+};
+constexpr int HIST_COLS = 11;
+
+struct SweepCtl {
+  double dt;
+  double frrot;
+  Body planet;
+  DevClock *clk;      // non-null: read dt/planet/frrot from the clock, honour halt
+  int fuse;           // sweepy epilogue: damping + CFL + finiteness check
+};
+
+}  // namespace pgd
+
+// launchers (pg_kernels.cu)
+namespace pgk {
+using namespace pgd;
+void tables(const Tables &T, const Phys &ph, int ndim, double kill_rin, double kill_rout, double xmin,
+            double xmax, cudaStream_t s);
+void sweep_x(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s);
+void sweep_y(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s);
+void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s);
+void cfl_full(const Tables &T, const double *r, const double *u, const double *v, const double *w,
+              const double *p0, const Phys &ph, double frrot, int ndim, unsigned long long *out,
+              cudaStream_t s);
+void index_shift(const Tables &T, double dt, double frrot, int fargo, const DevClock *clk, cudaStream_t s);
+void rotate(const Tables &T, const DevClock *clk, cudaStream_t s);
+void damp(const Tables &T, double *r, double *u, double *v, double *w, double dt, int ndim, cudaStream_t s);
+void reduce(const Tables &T, const double *r, const Body &pl, const DevClock *clk, double exclude,
+            int mode, int plnt, double p_alpha, int ndim, double *ring_part, unsigned int *counter,
+            double *out, double *hist_row, cudaStream_t s);
+void damp_clk(const Tables &T, double *r, double *u, double *v, double *w, const DevClock *clk,
+              cudaStream_t s);
+void cfl_clk(const Tables &T, const double *r, const double *u, const double *v, const double *w,
+             const Phys &ph, DevClock *clk, cudaStream_t s);
+void prestep(DevClock *clk, const Tables &T, int fargo, cudaStream_t s);
+void poststep(DevClock *clk, const Tables &T, cudaStream_t s);
+void record(DevClock *clk, cudaStream_t s);
+}  // namespace pgk

@@ -1,0 +1,199 @@
+// pg_ppm.cuh -- device side of one PPM Lagrange-remap pencil chunk.
+//
+// A chunk is 128 cells along the sweep direction: 116 interior cells plus 6
+// ghost cells on each side (n_pad 6, arrsize 128 of variable_types.h:13-16).
+// One thread owns one cell; the phases below are separated by CTA barriers
+// and read neighbours through shared memory.  Each phase keeps the index
+// range and the arithmetic order of the reference routine cited beside it,
+// so that the interior results agree with the reference to the last few
+// ulps (identical FMA contraction is the aim, not an assumption).
+//
+// Differences from the reference that do not change results:
+//  * chunks of a pencil are independent CTAs reading the pre-sweep state
+//    from a separate buffer, instead of one CTA walking the pencil with a
+//    6-cell carry (ppm.cu:43-157 carries pre-update values, so the result is
+//    the same Jacobi update);
+//  * the q = p/rho remap (remap.cu:291-300) is skipped: in EOS 0 the sweep
+//    store overwrites p with rho*cs2 (ppm.cu:139);
+//  * in 2D the w remap is skipped (w stays exactly 0) and umid *= pmid
+//    (evolve.cu:73, used by EOS 2 only) is dropped;
+//  * cs2(r) and nu(r) come from per-ring tables computed on the device with
+//    the same expressions.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pgd {
+
+constexpr int NPAD = 6;
+constexpr int ARR = 128;
+constexpr int REAL = ARR - 2 * NPAD;   // 116
+constexpr int AP = ARR + 2;            // padded shared length (flux[n+1] at n = 127)
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double kThird = 0.3333333333333333333333333;
+constexpr double kFourthd = 1.3333333333333333333333333;
+constexpr double kSmallp = 1.0e-15;
+constexpr double kSmallr = 1.0e-15;
+
+struct Body { double m, x, y, vx, vy, fx, fy, rs; };
+
+// Physics constants of the run (global.h), passed by value to kernels.
+struct Phys {
+  double gam, sc2, vis_nu, p_alpha, p_beta;
+  int plnt;       // plnt_flag > 0
+  int flat;       // flat_flag
+  int visc;       // visc_flag
+};
+
+struct Par { double c0, c1, c2, c3, c4; };
+
+// Shared arrays of one chunk: the sweep kernel's (ppm.cu:38-39) and
+// ppmlr's (ppmlr.cu:7-10).  q only serves as parabola storage (al) because
+// the q = p/rho remap is dead in EOS 0.
+struct ChunkShm {
+  double r[AP], p[AP], u[AP], v[AP], w[AP], xa0[AP], dx0[AP];
+  double q[AP], dx[AP], umid[AP], pmid[AP], tmp1[AP];
+};
+
+// ---- star + planet gravity, forces.cu:23-182 (non-barycentric frame) ------
+__device__ __forceinline__ double grav_rad_cyl(double rad, double azi, double z, const Body &p, double dt) {
+  double cosfac = cos(azi - (p.y + dt * p.vy));
+  double plm = p.m;
+  double plx = p.x;
+  double Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + z * z + p.rs * p.rs);
+  return -plm * (rad - plx * cosfac) / (Rp * Rp * Rp) - plm * cosfac / (plx * plx);
+}
+__device__ __forceinline__ double grav_azi_cyl(double rad, double azi, double z, const Body &p, double dt) {
+  double cosfac = cos(azi - (p.y + dt * p.vy));
+  double sinfac = sin(azi - (p.y + dt * p.vy));
+  double plm = p.m;
+  double plx = p.x;
+  double Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + z * z + p.rs * p.rs);
+  return -plm * plx * sinfac / (Rp * Rp * Rp) + plm * sinfac / plx / plx;
+}
+__device__ __forceinline__ double grav_rad_sph(double rad, double azi, double pol, const Body &p, double dt) {
+  double cosfac = cos(azi - (p.y + dt * p.vy));
+  double sinpol = sin(pol);
+  double stm = 1.0 / (1.0 + p.m);
+  double plm = p.m * stm;
+  double plx = p.x;
+  double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac * sinpol;
+  Rp = sqrt(Rp + p.rs * p.rs);
+  return -plm * (rad - plx * cosfac * sinpol) / (Rp * Rp * Rp) - stm / (rad * rad) - plm * sinpol * cosfac / (plx * plx);
+}
+__device__ __forceinline__ double grav_azi_sph(double rad, double azi, double pol, const Body &p, double dt) {
+  double cosfac = cos(azi - (p.y + dt * p.vy));
+  double sinfac = sin(azi - (p.y + dt * p.vy));
+  double sinpol = sin(pol);
+  rad /= sinpol;
+  double stm = 1.0 / (1.0 + p.m);
+  double plm = p.m * stm;
+  double plx = p.x;
+  double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac * sinpol;
+  Rp = sqrt(Rp + p.rs * p.rs);
+  return -plm * plx * sinfac / (Rp * Rp * Rp) + plm * sinpol * sinfac / plx / plx;
+}
+__device__ __forceinline__ double grav_pol_sph(double rad, double azi, double pol, const Body &p, double dt) {
+  double cosfac = cos(azi - (p.y + dt * p.vy));
+  double cospol = cos(pol);
+  double sinpol = sin(pol);
+  double stm = 1.0 / (1.0 + p.m);
+  double plm = p.m * stm;
+  double plx = p.x;
+  (void)stm;
+  double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac * sinpol;
+  Rp = sqrt(Rp + p.rs * p.rs);
+  return plm * plx * cosfac * cospol / (Rp * Rp * Rp) - plm * cosfac * cospol / (sinpol * plx * plx);
+}
+
+__device__ __forceinline__ double min3(double A, double B, double C) {   // simple_func.cu:2-14
+  if (A < B) { if (C < A) return C; else return A; }
+  else       { if (C < B) return C; else return B; }
+}
+__device__ __forceinline__ double max3(double A, double B, double C) {   // simple_func.cu:16-28
+  if (A > B) { if (C > A) return C; else return A; }
+  else       { if (C > B) return C; else return B; }
+}
+
+// paraset parabola.cu:236-274 (non-uniform PPM interface coefficients)
+__device__ __forceinline__ void paraset(int n, int nmin, int nmax, Par &par, const double *dx,
+                                        double *a, double *ai, double *b) {
+  double dx_n = 0.0, ain = 0.0, bi = 0.0, ci = 0.0, c = 0.0;
+  if (n >= nmin && n < nmax - 1) {
+    dx_n = dx[n];
+    double an = dx_n + dx[n + 1];
+    ain = 1.0 / an;
+    double bn = an + dx_n;
+    bi = 1.0 / bn;
+    c = an + dx[n + 1];
+    ci = 1.0 / c;
+    a[n] = an; ai[n] = ain; b[n] = bn;
+  }
+  __syncthreads();
+  if (n >= nmin + 1 && n < nmax - 2) {
+    double d = 1.0 / (a[n - 1] + a[n + 1]);
+    par.c0 = dx_n * ain * (1.0 + 2.0 * d * dx[n + 1] * (a[n - 1] * bi - a[n + 1] * ci));
+    par.c1 = -d * dx_n * a[n - 1] * bi;
+    par.c2 = d * dx[n + 1] * a[n + 1] * ci;
+  }
+  if (n >= nmin + 1 && n < nmax - 1) {
+    double d = dx_n / (a[n - 1] + dx[n + 1]);
+    par.c3 = d * b[n - 1] * ain;
+    par.c4 = d * c * ai[n - 1];
+  }
+  __syncthreads();
+}
+
+// parabola parabola.cu:168-231 (CW84 eq 1.5-1.8, 1.10)
+__device__ __forceinline__ void parabola(int n, int nmin, int nmax, double flat, const double *val,
+                                         double *al, double *da, double *a6, const Par &par) {
+  double t1 = 0.0, a = 0.0, ar = 0.0, da_r = 0.0;
+  if (n >= nmin + 1 && n < nmax - 1) {
+    a = val[n];
+    da_r = val[n + 1] - a;
+    double da_l = a - val[n - 1];
+    t1 = par.c3 * da_r + par.c4 * da_l;
+    if (t1 < 0.0) t1 = -min3(-t1, 2.0 * fabs(da_l), 2.0 * fabs(da_r));
+    else          t1 = min3(t1, 2.0 * fabs(da_l), 2.0 * fabs(da_r));
+    if (da_l * da_r < 0.0) t1 = 0.0;
+    a6[n] = t1;
+  }
+  __syncthreads();
+  if (n >= nmin + 1 && n < nmax - 2) {
+    ar = a + par.c0 * da_r + par.c1 * a6[n + 1] + par.c2 * t1;
+    al[n + 1] = ar;
+  }
+  __syncthreads();
+  if (n >= nmin + 2 && n < nmax - 2) {
+    double u1 = flat * a;
+    double u2 = 1.0 - flat;
+    double xr = u1 + u2 * ar;
+    double la = u1 + u2 * al[n];
+    u1 = xr - la;
+    u2 = u1 * u1;
+    u1 = u1 * (6.0 * (a - 0.5 * (xr + la)));
+    if ((xr - a) * (a - la) <= 0.0) { xr = a; la = a; }
+    if (u2 < u1) la = 3.0 * a - 2.0 * xr;
+    if (u2 < -u1) xr = 3.0 * a - 2.0 * la;
+    da[n] = xr - la;
+    a6[n] = 6.0 * (a - 0.5 * (xr + la));
+    al[n] = la;
+  }
+  __syncthreads();
+}
+
+// derivs viscosity.cu:2-18
+__device__ __forceinline__ void derivs(double &first, double &second, int n, const double *xf, const double *u) {
+  double x2 = xf[n] - xf[n - 1];
+  double x3 = xf[n + 1] - xf[n - 1];
+  double h2 = (u[n] - u[n - 1]) / x2;
+  double h3 = (u[n + 1] - u[n - 1]) / x3;
+  double A = (h3 - h2) / (x3 - x2);
+  double B = (x3 * h2 - x2 * h3) / (x3 - x2);
+  second = 2.0 * A;
+  first = second * x2 + B;
+}
+
+}  // namespace pgd

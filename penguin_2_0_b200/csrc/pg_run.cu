@@ -1,0 +1,796 @@
+// pg_run.cu -- the C ABI of include/penguin_b200.h: one disk run on one GPU.
+//
+// Device layout of a run (FP64, ring-major, physical azimuth order):
+//   planes  r, u (v_r), v (v_phi), w (v_theta, 3D only), two copies (A, B):
+//           [nk][nr + 12][nphi], rows 0..5 and nr+6..nr+11 are the fixed
+//           ghost rings lft/rgh (init.cpp:253-413), filled at load in both
+//           copies and never written by a sweep.  The radial sweep reads A
+//           and writes B, the azimuthal sweep reads B and writes A with the
+//           FARGO shift applied (so a 2D step ends back in A); the 3D polar
+//           sweep reads A and writes B, after which the copies swap roles.
+//   p       derived as r*cs2(r_cyl) (the EOS-0 store of ppm.cu:139); the
+//           pressure of a freshly loaded dump is kept in a plane `p0` that
+//           only the first radial sweep (and the first CFL) reads.
+//   tables  per radial row, per ring, per azimuth column, per polar layer.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pg_host.h"
+#include "pg_kernels.cuh"
+
+using pgd::NPAD;
+
+struct pg_run {
+  pg_params P{};
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int nr = 0, nphi = 0, nk = 0, nrg = 0;
+  size_t plane_elems = 0;
+  double *planes[2][4] = {{nullptr}};
+  double *p0 = nullptr;
+  bool p0_live = false;
+  int cur = 0;
+  // tables
+  double *tab = nullptr;
+  size_t tab_elems = 0;
+  int *itab = nullptr;
+  pgd::Tables T{};
+  pgd::Phys ph{};
+  // scratch + clock
+  double *ring_part = nullptr;
+  unsigned int *counter = nullptr;
+  double *dscal = nullptr;
+  unsigned long long *cfl = nullptr;
+  pgd::DevClock *clk = nullptr;
+  double *hist = nullptr;
+  int hist_cap = 4096;
+  // host side
+  std::vector<unsigned char> tmpl;   // last loaded dump (geometry fields)
+  std::vector<double> h_cs2;
+  bool loaded = false;
+  bool clock_ready = false;
+  int64_t launches = 0;
+  // captured step graphs
+  cudaGraphExec_t gexec = nullptr;
+  int gsteps = 0;
+};
+
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      run->err = std::string(#call) + ": " + cudaGetErrorString(e_);               \
+      return PG_ERR_CUDA;                                                          \
+    }                                                                              \
+  } while (0)
+
+static int fail(pg_run *run, int code, const std::string &msg) {
+  if (run) run->err = msg;
+  return code;
+}
+
+static int check_launch(pg_run *run, int n) {
+  run->launches += n;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    run->err = std::string("kernel launch: ") + cudaGetErrorString(e);
+    return PG_ERR_CUDA;
+  }
+  return PG_OK;
+}
+
+static pgd::Planes planes_fwd(pg_run *run, int src, const double *p0) {
+  pgd::Planes p;
+  p.r = run->planes[src][0]; p.u = run->planes[src][1]; p.v = run->planes[src][2]; p.w = run->planes[src][3];
+  p.ro = run->planes[1 - src][0]; p.uo = run->planes[1 - src][1]; p.vo = run->planes[1 - src][2];
+  p.wo = run->planes[1 - src][3];
+  p.p0 = p0;
+  return p;
+}
+
+extern "C" {
+
+const char *pg_last_error(const pg_run *run) { return run ? run->err.c_str() : "null run"; }
+
+int64_t pg_launch_count(const pg_run *run) { return run ? run->launches : 0; }
+
+int pg_create(const pg_params *p, int device, pg_run **out) {
+  if (!p || !out) return PG_ERR_ARG;
+  *out = nullptr;
+  std::string why;
+  int st = pg::check_params(p, why);
+  if (st) {
+    std::fprintf(stderr, "pg_create: %s\n", why.c_str());
+    return st;
+  }
+  pg_run *run = new pg_run();
+  run->P = *p;
+  run->dev = device;
+  run->nr = p->imax; run->nphi = p->jmax; run->nk = p->kmax; run->nrg = p->imax + 2 * NPAD;
+  auto bail = [&](int code) { pg_destroy(run); return code; };
+  if (cudaSetDevice(device) != cudaSuccess) { delete run; return PG_ERR_CUDA; }
+  if (cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PG_ERR_CUDA);
+  run->plane_elems = (size_t)run->nk * run->nrg * run->nphi;
+  int nf = (p->ndim == 3) ? 4 : 3;
+  for (int b = 0; b < 2; b++)
+    for (int f = 0; f < nf; f++)
+      if (cudaMalloc(&run->planes[b][f], run->plane_elems * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  if (cudaMalloc(&run->p0, run->plane_elems * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  // double tables
+  int nrg = run->nrg, nphi = run->nphi, nk = run->nk, nr = run->nr;
+  size_t nring = (size_t)nk * nrg;
+  size_t nz = (size_t)nk + 2 * NPAD;
+  run->tab_elems = 4 * (size_t)nrg + 10 * nring + 4 * (size_t)nphi + 4 * nz + (size_t)2 * NPAD * nr * 4;
+  if (cudaMalloc(&run->tab, run->tab_elems * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  if (cudaMalloc(&run->itab, 2 * nring * sizeof(int)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  double *t = run->tab;
+  pgd::Tables &T = run->T;
+  T.nr = nr; T.nphi = nphi; T.nk = nk; T.nrg = nrg;
+  T.cx = pgd::make_chunking(nr);
+  T.cy = pgd::make_chunking(nphi);
+  T.cz = pgd::make_chunking(nk);
+  T.rx = t; t += nrg; T.rdx = t; t += nrg; T.rxvol = t; t += nrg; T.rxc = t; t += nrg;
+  T.radc = t; t += nring; T.cs2 = t; t += nring; T.nu = t; t += nring; T.gp = t; t += nring;
+  T.val_r = t; t += nring; T.val_u = t; t += nring; T.val_v = t; t += nring;
+  T.damp_g = t; t += nring; T.damp_pw = t; t += nring;
+  T.res_v = t; t += nring;
+  // rot_v shares the block below (10th ring table)
+  T.y = t; t += nphi; T.dy = t; t += nphi; T.yvol = t; t += nphi; T.yc = t; t += nphi;
+  T.z = t; t += nz; T.dz = t; t += nz; T.zvol = t; t += nz; T.zc = t; t += nz;
+  T.tg = t; t += (size_t)2 * NPAD * nr * 4;
+  if (cudaMalloc(&T.rot_v, nring * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  T.inc_j = run->itab; T.rot_j = run->itab + nring;
+  // scratch
+  if (cudaMalloc(&run->ring_part, (size_t)nr * nk * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  if (cudaMalloc(&run->counter, sizeof(unsigned int)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  if (cudaMalloc(&run->dscal, 4 * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  if (cudaMalloc(&run->cfl, sizeof(unsigned long long)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  if (cudaMalloc(&run->clk, sizeof(pgd::DevClock)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  if (cudaMalloc(&run->hist, (size_t)run->hist_cap * pgd::HIST_COLS * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  if (cudaMemsetAsync(run->counter, 0, sizeof(unsigned int), run->stream) != cudaSuccess) return bail(PG_ERR_CUDA);
+  // physics constants
+  run->ph.gam = p->gam;
+  run->ph.sc2 = p->sc_h * p->sc_h;
+  run->ph.vis_nu = p->ss_alpha * p->sc_h * p->sc_h;
+  run->ph.p_alpha = p->p_alpha;
+  run->ph.p_beta = p->p_beta;
+  run->ph.plnt = p->plnt_flag > 0;
+  run->ph.flat = p->flat_flag != 0;
+  run->ph.visc = p->visc_flag == 1;
+  *out = run;
+  return PG_OK;
+}
+
+int pg_destroy(pg_run *run) {
+  if (!run) return PG_OK;
+  cudaSetDevice(run->dev);
+  if (run->stream) cudaStreamSynchronize(run->stream);
+  if (run->gexec) cudaGraphExecDestroy(run->gexec);
+  for (auto &b : run->planes)
+    for (auto &f : b) if (f) cudaFree(f);
+  cudaFree(run->p0);
+  cudaFree(run->tab);
+  cudaFree(run->itab);
+  cudaFree(run->T.rot_v);
+  cudaFree(run->ring_part);
+  cudaFree(run->counter);
+  cudaFree(run->dscal);
+  cudaFree(run->cfl);
+  cudaFree(run->clk);
+  cudaFree(run->hist);
+  if (run->stream) cudaStreamDestroy(run->stream);
+  delete run;
+  return PG_OK;
+}
+
+int pg_sync(pg_run *run) {
+  if (!run) return PG_ERR_ARG;
+  CK(cudaSetDevice(run->dev));
+  CK(cudaStreamSynchronize(run->stream));
+  return PG_OK;
+}
+
+// ---- load / save ----------------------------------------------------------------
+int pg_load_rings(pg_run *run, const void *rings, size_t bytes) {
+  if (!run || !rings) return PG_ERR_ARG;
+  const pg_params &P = run->P;
+  size_t rb = pg::ring_bytes(P.jmax);
+  if (bytes != rb * (size_t)P.imax * P.kmax)
+    return fail(run, PG_ERR_IO, "dump size does not match imax*kmax rings of 72*jmax+96 bytes");
+  CK(cudaSetDevice(run->dev));
+  const unsigned char *b = (const unsigned char *)rings;
+  pg::Geometry g;
+  std::string why;
+  int st = pg::read_geometry(P, b, g, why);
+  if (st) return fail(run, st, why);
+  pg::Profile pf{P};
+  std::vector<pg::SymDisk> val;
+  pg::build_val(pf, g.zxc, g.zzc, val);   // init_den/init_speed on the dump's grid
+  const int nr = run->nr, nphi = run->nphi, nk = run->nk, nrg = run->nrg;
+  const size_t nring = (size_t)nk * nrg, nz = (size_t)nk + 2 * NPAD;
+  // host images of the tables
+  std::vector<double> rx(nrg), rdx(nrg), rxvol(nrg), rxc(nrg);
+  std::vector<double> gp(nring, 0.0), vr(nring, 0.0), vu(nring, 0.0), vv(nring, 0.0);
+  std::vector<double> res_v(nring, 0.0), rot_v(nring, 0.0);
+  std::vector<int> inc_j(nring, 0), rot_j(nring, 0);
+  std::vector<double> z(nz, 0.0), dz(nz, 0.0), zvol(nz, 0.0), zc(nz, 0.0);
+  std::vector<double> tg((size_t)2 * NPAD * nr * 4, 0.0);
+  std::vector<pg::GhostRing> lft(NPAD * nk), rgh(NPAD * nk);
+  for (int i = 0; i < NPAD; i++)
+    for (int k = 0; k < nk; k++) {
+      double x = g.zxa[0] - g.zdx[0] * (double)(NPAD - i);
+      double dx = g.zdx[0];
+      lft[i + NPAD * k] = pg::make_ghost(pf, x, dx, x + 0.5 * dx, g.zza[k], g.zdz[k], g.zzc[k], 0);
+      x = g.zxa[nr - 1] + g.zdx[nr - 1] * (double)(i + 1);
+      dx = g.zdx[nr - 1];
+      rgh[i + NPAD * k] = pg::make_ghost(pf, x, dx, x + 0.5 * dx, g.zza[k], g.zdz[k], g.zzc[k], 0);
+    }
+  for (int i = 0; i < NPAD; i++) {
+    const pg::GhostRing &L = lft[i], &R = rgh[i];
+    rx[i] = L.x; rdx[i] = L.dx; rxvol[i] = L.xvol; rxc[i] = L.xc;
+    rx[nr + NPAD + i] = R.x; rdx[nr + NPAD + i] = R.dx; rxvol[nr + NPAD + i] = R.xvol; rxc[nr + NPAD + i] = R.xc;
+  }
+  for (int i = 0; i < nr; i++) {
+    rx[i + NPAD] = g.zxa[i]; rdx[i + NPAD] = g.zdx[i]; rxvol[i + NPAD] = g.xvol[i]; rxc[i + NPAD] = g.zxc[i];
+  }
+  for (int k = 0; k < nk; k++) {
+    for (int i = 0; i < NPAD; i++) {
+      size_t a = (size_t)k * nrg + i, c = (size_t)k * nrg + nr + NPAD + i;
+      gp[a] = lft[i + NPAD * k].p; rot_v[a] = lft[i + NPAD * k].rot_v;
+      gp[c] = rgh[i + NPAD * k].p; rot_v[c] = rgh[i + NPAD * k].rot_v;
+    }
+    for (int i = 0; i < nr; i++) {
+      size_t rk = (size_t)k * nrg + i + NPAD;
+      pg::RingView rv((unsigned char *)b + rb * (i + (size_t)nr * k), nphi);
+      rot_v[rk] = *rv.rot(0); res_v[rk] = *rv.rot(1);
+      rot_j[rk] = *rv.rj(0); inc_j[rk] = *rv.rj(1);
+      if (rot_j[rk] < 0 || rot_j[rk] >= nphi) return fail(run, PG_ERR_STATE, "rot_j out of range in dump");
+      const pg::SymDisk &sv = val[i + (size_t)nr * k];
+      vr[rk] = sv.r; vu[rk] = sv.u; vv[rk] = sv.v;
+    }
+  }
+  // polar layers: lower ghosts (udr geometry), interior, upper ghosts (top geometry)
+  for (int kk = 0; kk < NPAD; kk++) {
+    double zl = g.zza[0] - g.zdz[0] * (double)(NPAD - kk), dzl = g.zdz[0];
+    z[kk] = zl; dz[kk] = dzl; zc[kk] = zl + 0.5 * dzl; zvol[kk] = pf.vol(zl, dzl, 2);
+    double zu = g.zza[nk - 1] + g.zdz[nk - 1] * (double)(kk + 1), dzu = g.zdz[nk - 1];
+    size_t q = nk + NPAD + kk;
+    z[q] = zu; dz[q] = dzu; zc[q] = zu + 0.5 * dzu; zvol[q] = pf.vol(zu, dzu, 2);
+  }
+  for (int k = 0; k < nk; k++) {
+    z[k + NPAD] = g.zza[k]; dz[k + NPAD] = g.zdz[k]; zvol[k + NPAD] = g.zvol[k]; zc[k + NPAD] = g.zzc[k];
+  }
+  if (P.ndim == 3) {
+    for (int kk = 0; kk < NPAD; kk++)
+      for (int i = 0; i < nr; i++) {
+        pg::GhostRing u = pg::make_ghost(pf, g.zxa[i], g.zdx[i], g.zxc[i], z[kk], dz[kk], zc[kk], 1);
+        double *q = &tg[((size_t)kk * nr + i) * 4];
+        q[0] = u.r; q[1] = u.p; q[2] = u.u; q[3] = u.v;
+        size_t qi = NPAD + kk;
+        pg::GhostRing tp = pg::make_ghost(pf, g.zxa[i], g.zdx[i], g.zxc[i], z[nk + NPAD + kk], dz[nk + NPAD + kk],
+                                          zc[nk + NPAD + kk], 1);
+        q = &tg[(qi * nr + i) * 4];
+        q[0] = tp.r; q[1] = tp.p; q[2] = tp.u; q[3] = tp.v;
+      }
+  }
+  // planes in physical azimuth order
+  const size_t pe = run->plane_elems;
+  std::vector<double> hr(pe), hu(pe), hv(pe), hw(P.ndim == 3 ? pe : 0), hp(pe, 0.0);
+  for (int k = 0; k < nk; k++) {
+    for (int gi = 0; gi < NPAD; gi++) {
+      const pg::GhostRing *gs[2] = {&lft[gi + NPAD * k], &rgh[gi + NPAD * k]};
+      int rows[2] = {gi, nr + NPAD + gi};
+      for (int s = 0; s < 2; s++) {
+        size_t off = ((size_t)k * nrg + rows[s]) * nphi;
+        for (int j = 0; j < nphi; j++) {
+          hr[off + j] = gs[s]->r; hu[off + j] = gs[s]->u; hv[off + j] = gs[s]->v; hp[off + j] = gs[s]->p;
+          if (P.ndim == 3) hw[off + j] = 0.0;
+        }
+      }
+    }
+    for (int i = 0; i < nr; i++) {
+      size_t rk = (size_t)k * nrg + i + NPAD;
+      size_t off = rk * nphi;
+      pg::RingView rv((unsigned char *)b + rb * (i + (size_t)nr * k), nphi);
+      int rj = rot_j[rk];
+      for (int js = 0; js < nphi; js++) {
+        int jp = js + rj;
+        if (jp >= nphi) jp -= nphi;
+        hr[off + jp] = rv.f(0)[js];
+        hp[off + jp] = rv.f(1)[js];
+        hu[off + jp] = rv.f(2)[js];
+        hv[off + jp] = rv.f(3)[js];
+        double w = rv.f(4)[js];
+        if (P.ndim == 3) hw[off + jp] = w;
+        else if (w != 0.0) return fail(run, PG_ERR_STATE, "2D dump with nonzero w");
+        if (!(rv.f(0)[js] > 0.0) || !std::isfinite(rv.f(0)[js])) return fail(run, PG_ERR_STATE, "non-positive density in dump");
+      }
+    }
+  }
+  cudaStream_t s = run->stream;
+  pgd::Tables &T = run->T;
+  auto up = [&](const double *dst, const std::vector<double> &src) {
+    return cudaMemcpyAsync((void *)dst, src.data(), src.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+  };
+  CK(up(T.rx, rx)); CK(up(T.rdx, rdx)); CK(up(T.rxvol, rxvol)); CK(up(T.rxc, rxc));
+  CK(up(T.gp, gp)); CK(up(T.val_r, vr)); CK(up(T.val_u, vu)); CK(up(T.val_v, vv));
+  CK(up(T.res_v, res_v)); CK(up(T.rot_v, rot_v));
+  CK(cudaMemcpyAsync(T.inc_j, inc_j.data(), nring * sizeof(int), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(T.rot_j, rot_j.data(), nring * sizeof(int), cudaMemcpyHostToDevice, s));
+  CK(up(T.y, g.zya)); CK(up(T.dy, g.zdy)); CK(up(T.yvol, g.yvol)); CK(up(T.yc, g.zyc));
+  CK(up(T.z, z)); CK(up(T.dz, dz)); CK(up(T.zvol, zvol)); CK(up(T.zc, zc));
+  CK(up(T.tg, tg));
+  for (int bsel = 0; bsel < 2; bsel++) {
+    CK(cudaMemcpyAsync(run->planes[bsel][0], hr.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(run->planes[bsel][1], hu.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(run->planes[bsel][2], hv.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (P.ndim == 3)
+      CK(cudaMemcpyAsync(run->planes[bsel][3], hw.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaMemcpyAsync(run->p0, hp.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+  pgk::tables(T, run->ph, P.ndim, P.kill_rin, P.kill_rout, P.xmin, P.xmax, s);
+  if (int e = check_launch(run, 1)) return e;
+  CK(cudaStreamSynchronize(s));
+  run->h_cs2.resize(nring);
+  CK(cudaMemcpy(run->h_cs2.data(), T.cs2, nring * sizeof(double), cudaMemcpyDeviceToHost));
+  run->tmpl.assign(b, b + bytes);
+  run->cur = 0;
+  run->p0_live = true;
+  run->loaded = true;
+  run->clock_ready = false;
+  if (run->gexec) { cudaGraphExecDestroy(run->gexec); run->gexec = nullptr; run->gsteps = 0; }
+  return PG_OK;
+}
+
+int pg_load_dump(pg_run *run, const char *path) {
+  if (!run || !path) return PG_ERR_ARG;
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(run, PG_ERR_IO, std::string("cannot open ") + path);
+  size_t want = pg::ring_bytes(run->P.jmax) * (size_t)run->P.imax * run->P.kmax;
+  std::vector<unsigned char> buf(want);
+  size_t got = std::fread(buf.data(), 1, want, f);
+  int extra = std::fgetc(f);
+  std::fclose(f);
+  if (got != want || extra != EOF) return fail(run, PG_ERR_IO, "dump file size does not match the grid");
+  return pg_load_rings(run, buf.data(), want);
+}
+
+int pg_save_rings(pg_run *run, void *rings, size_t bytes) {
+  if (!run || !rings) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  const pg_params &P = run->P;
+  size_t rb = pg::ring_bytes(P.jmax);
+  if (bytes != rb * (size_t)P.imax * P.kmax) return fail(run, PG_ERR_ARG, "buffer size mismatch");
+  CK(cudaSetDevice(run->dev));
+  const int nr = run->nr, nphi = run->nphi, nk = run->nk, nrg = run->nrg;
+  const size_t nring = (size_t)nk * nrg, pe = run->plane_elems;
+  std::vector<double> hr(pe), hu(pe), hv(pe), hw(P.ndim == 3 ? pe : 0), hp;
+  std::vector<double> res_v(nring), rot_v(nring);
+  std::vector<int> inc_j(nring), rot_j(nring);
+  cudaStream_t s = run->stream;
+  double **cp = run->planes[run->cur];
+  CK(cudaMemcpyAsync(hr.data(), cp[0], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hu.data(), cp[1], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hv.data(), cp[2], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (P.ndim == 3) CK(cudaMemcpyAsync(hw.data(), cp[3], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (run->p0_live) {
+    hp.resize(pe);
+    CK(cudaMemcpyAsync(hp.data(), run->p0, pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaMemcpyAsync(res_v.data(), run->T.res_v, nring * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(rot_v.data(), run->T.rot_v, nring * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(inc_j.data(), run->T.inc_j, nring * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(rot_j.data(), run->T.rot_j, nring * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  unsigned char *out = (unsigned char *)rings;
+  std::memcpy(out, run->tmpl.data(), bytes);
+  for (int k = 0; k < nk; k++)
+    for (int i = 0; i < nr; i++) {
+      size_t rk = (size_t)k * nrg + i + NPAD, off = rk * nphi;
+      pg::RingView rv(out + rb * (i + (size_t)nr * k), nphi);
+      int rj = rot_j[rk];
+      double c2 = run->h_cs2[rk];
+      for (int js = 0; js < nphi; js++) {
+        int jp = js + rj;
+        if (jp >= nphi) jp -= nphi;
+        double r = hr[off + jp];
+        rv.f(0)[js] = r;
+        rv.f(1)[js] = run->p0_live ? hp[off + jp] : r * c2;   // EOS-0 store, ppm.cu:139
+        rv.f(2)[js] = hu[off + jp];
+        rv.f(3)[js] = hv[off + jp];
+        rv.f(4)[js] = (P.ndim == 3) ? hw[off + jp] : 0.0;
+      }
+      *rv.rot(0) = rot_v[rk]; *rv.rot(1) = res_v[rk];
+      *rv.rj(0) = rot_j[rk]; *rv.rj(1) = inc_j[rk];
+    }
+  return PG_OK;
+}
+
+int pg_save_dump(pg_run *run, const char *path) {
+  if (!run || !path) return PG_ERR_ARG;
+  size_t bytes = pg::ring_bytes(run->P.jmax) * (size_t)run->P.imax * run->P.kmax;
+  std::vector<unsigned char> buf(bytes);
+  int st = pg_save_rings(run, buf.data(), bytes);
+  if (st) return st;
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return fail(run, PG_ERR_IO, std::string("cannot write ") + path);
+  size_t w = std::fwrite(buf.data(), 1, bytes, f);
+  std::fclose(f);
+  return (w == bytes) ? PG_OK : fail(run, PG_ERR_IO, "short write");
+}
+
+int pg_device_view_get(pg_run *run, pg_device_view *v) {
+  if (!run || !v) return PG_ERR_ARG;
+  double **cp = run->planes[run->cur];
+  v->sigma = cp[0] + (size_t)NPAD * run->nphi;
+  v->vr = cp[1] + (size_t)NPAD * run->nphi;
+  v->vphi = cp[2] + (size_t)NPAD * run->nphi;
+  v->row_stride = run->nphi;
+  v->imax = run->nr; v->jmax = run->nphi; v->kmax = run->nk;
+  v->pad = run->nrg;
+  v->stream = (void *)run->stream;
+  return PG_OK;
+}
+
+// ---- the reference's entry points ---------------------------------------------
+int pg_get_dt(pg_run *run, double dt_old, double frrot, double *dt_out) {
+  if (!run || !dt_out) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  CK(cudaSetDevice(run->dev));
+  cudaStream_t s = run->stream;
+  double **cp = run->planes[run->cur];
+  CK(cudaMemsetAsync(run->cfl, 0, sizeof(unsigned long long), s));
+  pgk::cfl_full(run->T, cp[0], cp[1], cp[2], cp[3], run->p0_live ? run->p0 : nullptr, run->ph, frrot,
+                run->P.ndim, run->cfl, s);
+  if (int e = check_launch(run, 1)) return e;
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, run->cfl, sizeof(bits), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double rate;
+  std::memcpy(&rate, &bits, sizeof(rate));
+  double h = run->P.courant / rate;       // dt_lv3 timestep.cu:105
+  double dt = 1.1 * dt_old;               // timestep.cu:135-141
+  dt = (h < dt) ? h : dt;
+  *dt_out = dt;
+  if (dt / run->P.endtime < 1.0e-12) return fail(run, PG_ERR_DT_COLLAPSE, "time step too small");
+  return PG_OK;
+}
+
+int pg_index_shift(pg_run *run, double dt, double frrot) {
+  if (!run) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  CK(cudaSetDevice(run->dev));
+  pgk::index_shift(run->T, dt, frrot, run->P.FARGO_flag, nullptr, run->stream);
+  return check_launch(run, 1);
+}
+
+static pgd::SweepCtl host_ctl(double dt, const pg_body *pl, double frrot) {
+  pgd::SweepCtl c{};
+  c.dt = dt;
+  c.frrot = frrot;
+  c.planet = pgd::Body{pl->m, pl->x, pl->y, pl->vx, pl->vy, pl->fx, pl->fy, pl->rs};
+  c.clk = nullptr;
+  c.fuse = 0;
+  return c;
+}
+
+int pg_sweep2d(pg_run *run, double dt, const pg_body *planet, double frrot) {
+  if (!run || !planet) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  if (run->P.ndim != 2) return fail(run, PG_ERR_PARAMS, "pg_sweep2d on a 3D run");
+  CK(cudaSetDevice(run->dev));
+  pgd::SweepCtl c = host_ctl(dt, planet, frrot);
+  cudaStream_t s = run->stream;
+  pgk::sweep_x(run->T, planes_fwd(run, run->cur, run->p0_live ? run->p0 : nullptr), run->ph, c, 2, s);
+  pgk::sweep_y(run->T, planes_fwd(run, 1 - run->cur, nullptr), run->ph, c, 2, s);
+  if (run->P.FARGO_flag > 0) pgk::rotate(run->T, nullptr, s);
+  run->p0_live = false;
+  return check_launch(run, run->P.FARGO_flag > 0 ? 3 : 2);
+}
+
+int pg_sweep3d(pg_run *run, double dt, const pg_body *planet, double frrot) {
+  if (!run || !planet) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  if (run->P.ndim != 3) return fail(run, PG_ERR_PARAMS, "pg_sweep3d on a 2D run");
+  CK(cudaSetDevice(run->dev));
+  pgd::SweepCtl c = host_ctl(dt, planet, frrot);
+  cudaStream_t s = run->stream;
+  int a = run->cur;
+  pgk::sweep_x(run->T, planes_fwd(run, a, run->p0_live ? run->p0 : nullptr), run->ph, c, 3, s);
+  pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 3, s);
+  pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, run->P.ntop, s);
+  if (run->P.FARGO_flag > 0) pgk::rotate(run->T, nullptr, s);
+  run->cur = 1 - a;
+  run->p0_live = false;
+  return check_launch(run, run->P.FARGO_flag > 0 ? 4 : 3);
+}
+
+int pg_damp(pg_run *run, double dt) {
+  if (!run) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  CK(cudaSetDevice(run->dev));
+  double **cp = run->planes[run->cur];
+  pgk::damp(run->T, cp[0], cp[1], cp[2], cp[3], dt, run->P.ndim, run->stream);
+  return check_launch(run, 1);
+}
+
+int pg_reduce(pg_run *run, const pg_body *planet, double exclude, int mode, double *out) {
+  if (!run || !planet || !out) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  if (mode != 0 && mode != 8 && mode != 9) return fail(run, PG_ERR_ARG, "mode must be 0, 8 or 9");
+  if (run->P.ndim == 3 && run->nk > 64) return fail(run, PG_ERR_PARAMS, "3D reductions support kmax <= 64");
+  CK(cudaSetDevice(run->dev));
+  pgd::Body b{planet->m, planet->x, planet->y, planet->vx, planet->vy, planet->fx, planet->fy, planet->rs};
+  exclude *= run->P.sc_h;                                 // device_func.cu:171
+  pgk::reduce(run->T, run->planes[run->cur][0], b, nullptr, exclude, mode, run->P.plnt_flag > 0,
+              run->P.p_alpha, run->P.ndim, run->ring_part, run->counter, run->dscal, nullptr, run->stream);
+  if (int e = check_launch(run, 1)) return e;
+  CK(cudaMemcpyAsync(out, run->dscal, sizeof(double), cudaMemcpyDeviceToHost, run->stream));
+  CK(cudaStreamSynchronize(run->stream));
+  *out = 0.0 + *out;                                       // host sum device_func.cu:195
+  return PG_OK;
+}
+
+// ---- planet, planet.cu:11-93 (host arithmetic as in the reference) --------------
+double pg_set_M_p(const pg_params *p, double t) {
+  if (t < p->t_growth) return std::fmax(p->M_p * std::sin(pg::kPi * t / (2.0 * p->t_growth)), 0.01 * pg::kEarthMass);
+  return p->M_p;
+}
+
+int pg_init_planet(const pg_params *p, pg_body *pl, double *frrot) {
+  if (!p || !pl || !frrot) return PG_ERR_ARG;
+  pg::Profile pf{*p};
+  pl->m = pg_set_M_p(p, 0.0);
+  pl->x = p->R_p;
+  pl->y = pg::kPi;
+  pl->vx = 0.0;
+  pl->vy = std::pow(pl->x, -1.5);
+  *frrot = (p->FrRot_flag == 1) ? pl->vy : 0.0;
+  pl->vy -= *frrot;
+  pl->rs = p->rs_fac * pf.h(pl->x);
+  pl->fx = 0.0; pl->fy = 0.0;
+  return PG_OK;
+}
+
+int pg_planet_forces(pg_run *run, pg_body *pl, double frrot, double simtime) {
+  if (!run || !pl) return PG_ERR_ARG;
+  const pg_params &P = run->P;
+  pl->m = pg_set_M_p(&P, simtime);
+  if (P.plnt_flag == 2) {
+    double f8 = 0.0, f9 = 0.0;
+    int st = pg_reduce(run, pl, 0.0, 8, &f8);
+    if (st) return st;
+    pl->fx = P.Sigma_0 * f8 / pl->m - 1.0 / pl->x / pl->x + pl->x * std::pow(pl->vy + frrot, 2);
+    st = pg_reduce(run, pl, 0.0, 9, &f9);
+    if (st) return st;
+    pl->fy = P.Sigma_0 * f9 / pl->m;
+  } else {
+    pl->fx = -1.0 / pl->x / pl->x + pl->x * std::pow(pl->vy + frrot, 2);
+    pl->fy = 0.0;
+  }
+  return PG_OK;
+}
+
+int pg_kick_drift_kick(const pg_params *p, pg_body *pl, double *frrot, double dt, int kick) {
+  if (!p || !pl || !frrot) return PG_ERR_ARG;
+  if (!kick) {
+    pg::Profile pf{*p};
+    double old_rad = pl->x;
+    pl->x += dt * pl->vx;
+    pl->y += dt * pl->vy;
+    pl->vy = ((pl->vy + *frrot) * old_rad * old_rad / pl->x / pl->x) - *frrot;
+    if (pl->y < 0.0) pl->y += pg::kTwoPi;
+    if (pl->y >= pg::kTwoPi) pl->y -= pg::kTwoPi;
+    pl->rs = p->rs_fac * pf.h(pl->x);
+  } else {
+    pl->vx += dt * pl->fx;
+    pl->vy += *frrot + dt * pl->fy / pl->x / pl->x;
+    *frrot = (p->FrRot_flag == 1) ? pl->vy : 0.0;
+    pl->vy -= *frrot;
+  }
+  return PG_OK;
+}
+
+double pg_get_E(const pg_body *p, double frrot) {
+  double vy = p->vy + frrot;
+  return (p->vx * p->vx + vy * vy * p->x * p->x) / 2.0 - 1.0 / p->x;
+}
+
+double pg_get_ecc(const pg_body *p, double frrot) {
+  double vy = p->vy + frrot;
+  double L = vy * p->x * p->x;
+  return std::sqrt(1.0 + (2.0 * pg_get_E(p, frrot) * L * L));
+}
+
+// ---- fused device-resident loop --------------------------------------------------
+int pg_clock_reset(pg_run *run, int startat) {
+  if (!run) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  const pg_params &P = run->P;
+  if (P.plnt_flag == 2) return fail(run, PG_ERR_PARAMS, "the fused loop supports plnt_flag 0 and 1");
+  if (P.ndim == 3 && run->nk > 64) return fail(run, PG_ERR_PARAMS, "3D diagnostics support kmax <= 64");
+  CK(cudaSetDevice(run->dev));
+  pgd::DevClock c{};
+  c.simtime = P.tmovie * (double)startat;                 // main.cu:272
+  c.timem = 0.0;
+  c.dt = P.endtime;                                       // main.cu:270
+  c.endtime = P.endtime; c.tmovie = P.tmovie; c.courant = P.courant;
+  pg_body b;
+  double fr;
+  pg_init_planet(&P, &b, &fr);                            // main.cu:327
+  if (int st = pg_planet_forces(run, &b, fr, c.simtime)) return st;  // main.cu:328
+  c.planet = pgd::Body{b.m, b.x, b.y, b.vx, b.vy, b.fx, b.fy, b.rs};
+  c.frrot = fr; c.frrot_next = fr;
+  c.ncycle = 0; c.ncycp = 0; c.ncycend = P.ncycend;
+  c.nprin = P.nprin; c.plnt_flag = P.plnt_flag; c.frrot_flag = P.FrRot_flag; c.ndim = P.ndim;
+  c.M_p = P.M_p; c.t_growth = P.t_growth; c.rs_fac = P.rs_fac; c.sc2 = P.sc_h * P.sc_h; c.R_p = P.R_p;
+  c.Sigma_0 = P.Sigma_0;
+  c.hist_norm = P.M_p * P.M_p * std::pow(P.R_p, 1.0 - P.p_alpha + (P.p_beta - 1.0)) / (P.sc_h * P.sc_h);
+  c.hist = run->hist; c.hist_cap = run->hist_cap; c.hist_count = 0;
+  cudaStream_t s = run->stream;
+  CK(cudaMemcpyAsync(run->clk, &c, sizeof(c), cudaMemcpyHostToDevice, s));
+  // first get_dt's CFL rate (the fused loop takes later ones from sweepy)
+  double **cp = run->planes[run->cur];
+  pgk::cfl_full(run->T, cp[0], cp[1], cp[2], cp[3], run->p0_live ? run->p0 : nullptr, run->ph, fr, P.ndim,
+                &run->clk->cfl_bits, s);
+  if (int e = check_launch(run, 1)) return e;
+  CK(cudaStreamSynchronize(s));
+  run->clock_ready = true;
+  return PG_OK;
+}
+
+int pg_clock_get(pg_run *run, pg_clock *out, pg_body *planet) {
+  if (!run) return PG_ERR_ARG;
+  if (!run->clock_ready) return fail(run, PG_ERR_STATE, "clock not reset");
+  CK(cudaSetDevice(run->dev));
+  pgd::DevClock c;
+  CK(cudaMemcpyAsync(&c, run->clk, sizeof(c), cudaMemcpyDeviceToHost, run->stream));
+  CK(cudaStreamSynchronize(run->stream));
+  if (out) {
+    out->simtime = c.simtime; out->timem = c.timem; out->dt = c.dt; out->dt_used = c.dt_step;
+    out->frrot = c.frrot; out->ncycle = c.ncycle; out->make_pict = c.make_pict; out->done = c.done;
+    out->status = c.status; out->pad = c.halted;
+  }
+  if (planet) {
+    planet->m = c.planet.m; planet->x = c.planet.x; planet->y = c.planet.y; planet->vx = c.planet.vx;
+    planet->vy = c.planet.vy; planet->fx = c.planet.fx; planet->fy = c.planet.fy; planet->rs = c.planet.rs;
+  }
+  return PG_OK;
+}
+
+// one step of main.cu:343-441 as device work on the run's stream
+static int enqueue_step(pg_run *run, bool first_p0) {
+  const pg_params &P = run->P;
+  cudaStream_t s = run->stream;
+  pgd::SweepCtl c{};
+  c.clk = run->clk;
+  c.fuse = 0;
+  int a = run->cur;
+  int n = 0;
+  pgk::prestep(run->clk, run->T, P.FARGO_flag, s); n++;
+  pgk::sweep_x(run->T, planes_fwd(run, a, first_p0 ? run->p0 : nullptr), run->ph, c, P.ndim, s); n++;
+  if (P.ndim == 2) {
+    c.fuse = 1;
+    pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 2, s); n++;
+  } else {
+    pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 3, s); n++;
+    // 3D: damping and CFL after the polar sweep
+    pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, P.ntop, s); n++;
+    double **cp = run->planes[1 - a];
+    pgk::damp_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->clk, s); n++;
+    pgk::cfl_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->ph, run->clk, s); n++;
+    run->cur = 1 - a;
+  }
+  pgk::poststep(run->clk, run->T, s); n++;
+  if (P.plnt_flag > 0 || true) {
+    double **cp = run->planes[run->cur];
+    pgk::reduce(run->T, cp[0], pgd::Body{}, run->clk, 0.0, 0, P.plnt_flag > 0, P.p_alpha, P.ndim,
+                run->ring_part, run->counter, &run->clk->mass, nullptr, s); n++;
+    if (P.plnt_flag > 0 && P.ndim == 2) {
+      pgk::reduce(run->T, cp[0], pgd::Body{}, run->clk, 0.0, 9, 1, P.p_alpha, P.ndim, run->ring_part,
+                  run->counter, &run->clk->torque, nullptr, s); n++;
+    }
+    pgk::record(run->clk, s); n++;
+  }
+  return check_launch(run, n);
+}
+
+static int finish_advance(pg_run *run, int64_t before, int *taken) {
+  pgd::DevClock c;
+  CK(cudaMemcpyAsync(&c, run->clk, sizeof(c), cudaMemcpyDeviceToHost, run->stream));
+  CK(cudaStreamSynchronize(run->stream));
+  if (taken) *taken = (int)(c.ncycle - before);
+  if (c.status != 0) {
+    return fail(run, c.status, c.status == PG_ERR_NONFINITE ? "non-finite or non-positive state"
+                                                           : "time step collapsed");
+  }
+  if (c.halted && !c.done) {
+    // landed on tmovie: let the caller dump, then continue
+    int zero = 0;
+    CK(cudaMemcpyAsync(&run->clk->halted, &zero, sizeof(int), cudaMemcpyHostToDevice, run->stream));
+    CK(cudaStreamSynchronize(run->stream));
+  }
+  return PG_OK;
+}
+
+int pg_advance(pg_run *run, int nsteps, int *taken) {
+  if (!run) return PG_ERR_ARG;
+  if (!run->clock_ready) return fail(run, PG_ERR_STATE, "call pg_clock_reset first");
+  CK(cudaSetDevice(run->dev));
+  pgd::DevClock c;
+  CK(cudaMemcpy(&c, run->clk, sizeof(c), cudaMemcpyDeviceToHost));
+  int64_t before = c.ncycle;
+  for (int i = 0; i < nsteps; i++) {
+    bool first = run->p0_live;
+    if (int e = enqueue_step(run, first)) return e;
+    run->p0_live = false;
+  }
+  return finish_advance(run, before, taken);
+}
+
+int pg_advance_graph(pg_run *run, int nsteps, int chunk, int *taken) {
+  if (!run) return PG_ERR_ARG;
+  if (!run->clock_ready) return fail(run, PG_ERR_STATE, "call pg_clock_reset first");
+  if (chunk < 1) return fail(run, PG_ERR_ARG, "chunk must be >= 1");
+  CK(cudaSetDevice(run->dev));
+  if (run->P.ndim == 3 && (chunk & 1)) chunk += 1;   // 3D steps alternate the plane copies
+  pgd::DevClock c;
+  CK(cudaMemcpy(&c, run->clk, sizeof(c), cudaMemcpyDeviceToHost));
+  int64_t before = c.ncycle;
+  int done = 0;
+  if (run->p0_live && nsteps > 0) {
+    if (int e = enqueue_step(run, true)) return e;
+    run->p0_live = false;
+    done = 1;
+  }
+  if (!run->gexec || run->gsteps != chunk) {
+    if (run->gexec) { cudaGraphExecDestroy(run->gexec); run->gexec = nullptr; }
+    int cur0 = run->cur;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(run->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < chunk; i++) {
+      int e = enqueue_step(run, false);
+      if (e) { cudaStreamEndCapture(run->stream, &g); return e; }
+    }
+    CK(cudaStreamEndCapture(run->stream, &g));
+    CK(cudaGraphInstantiate(&run->gexec, g, 0));
+    cudaGraphDestroy(g);
+    run->gsteps = chunk;
+    run->cur = cur0;
+    run->launches -= 0;
+  }
+  int64_t per = 0;
+  for (; done + chunk <= nsteps; done += chunk) {
+    CK(cudaGraphLaunch(run->gexec, run->stream));
+    per++;
+  }
+  for (; done < nsteps; done++) {
+    if (int e = enqueue_step(run, false)) return e;
+  }
+  (void)per;
+  return finish_advance(run, before, taken);
+}
+
+int pg_history(pg_run *run, double *rows, int max, int *rows_out) {
+  if (!run || !rows_out) return PG_ERR_ARG;
+  if (!run->clock_ready) return fail(run, PG_ERR_STATE, "clock not reset");
+  CK(cudaSetDevice(run->dev));
+  pgd::DevClock c;
+  CK(cudaMemcpyAsync(&c, run->clk, sizeof(c), cudaMemcpyDeviceToHost, run->stream));
+  CK(cudaStreamSynchronize(run->stream));
+  int n = c.hist_count < max ? c.hist_count : max;
+  if (n > 0 && rows)
+    CK(cudaMemcpy(rows, run->hist, (size_t)n * pgd::HIST_COLS * sizeof(double), cudaMemcpyDeviceToHost));
+  int zero = 0;
+  CK(cudaMemcpy(&run->clk->hist_count, &zero, sizeof(int), cudaMemcpyHostToDevice));
+  *rows_out = n;
+  return PG_OK;
+}
+
+}  // extern "C"

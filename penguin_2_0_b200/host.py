@@ -1,0 +1,339 @@
+"""Host-side mirror of the reference's hydro-step interface.
+
+The reference exposes its hot path as C++ functions called from main.cu's
+time loop.  This module gives the same names, argument meaning and order over
+the C ABI of libpenguin_b200.so, so a caller (or a test) reads like the
+reference's own driver:
+
+    reference (file:line)                          here
+    bundle_sweep2D(set, dt, planet, FrRot)         bundle_sweep2D(run, dt, planet, FrRot)
+      include/ppm.h:4, src/ppm/ppm.cu:358
+    get_dt(dt, set, FrRot)                         get_dt(dt, run, FrRot)
+      include/timestep.h:4, timestep.cu:112
+    Index_Shift(set, dt, FrRot)                    Index_Shift(run, dt, FrRot)
+      include/orbital_advection.h:4, orbital_advection.cu:45
+    GPU_output_reduction(set, planet, exclude, m)  GPU_output_reduction(run, planet, exclude, m)
+      include/output.h:32, device_func.cu:169
+    init_planet / planet_forces / kick_drift_kick  same names, planet.cu:36-93
+    kernel() time loop main.cu:343-441             Run.kernel_loop(nsteps) (host-driven)
+                                                   Run.advance(nsteps) (device-resident)
+
+Errors: every call raises PenguinError carrying the C status and message
+(the reference prints and exits, include/cuSafe.cu:8-47).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import pg_body, pg_clock, pg_params
+
+TWOPI = 6.283185307179586476925286766559
+HIST_COLS = 11
+
+
+class PenguinError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_lib.STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _check(st: int, run=None, what: str = ""):
+    if st != 0:
+        msg = what
+        if run is not None and getattr(run, "_h", None):
+            m = _lib.lib().pg_last_error(run._h)
+            msg = f"{what}: {m.decode() if m else ''}"
+        raise PenguinError(st, msg)
+
+
+def params(which: int | None = None, **over) -> pg_params:
+    """pg_params of a named workload (0: 2D 256x768, 1: 3D 128x1024x32,
+    2: 2D 1024x3072) or of the reference defaults (which=None)."""
+    p = pg_params()
+    L = _lib.lib()
+    _check(L.pg_default_params(C.byref(p)) if which is None else L.pg_config_params(which, C.byref(p)),
+           what="params")
+    p.update(**over)
+    return p
+
+
+def check_params(p: pg_params) -> int:
+    return _lib.lib().pg_check_params(C.byref(p))
+
+
+def ring_bytes(jmax: int) -> int:
+    return _lib.lib().pg_ring_bytes(jmax)
+
+
+def build_ic(p: pg_params) -> bytearray:
+    """Seeded initial condition in the reference dump layout."""
+    n = ring_bytes(p.jmax) * p.imax * p.kmax
+    buf = bytearray(n)
+    cbuf = (C.c_char * n).from_buffer(buf)
+    _check(_lib.lib().pg_build_ic(C.byref(p), cbuf, n), what="pg_build_ic")
+    return buf
+
+
+def label(p: pg_params) -> str:
+    b = C.create_string_buffer(256)
+    _check(_lib.lib().pg_label(C.byref(p), b, 256), what="pg_label")
+    return b.value.decode()
+
+
+# ---- dump layout (variable_types.h:67-97) ---------------------------------------
+def dump_fields(buf, p: pg_params) -> dict:
+    """Views of a dump image: r,p,u,v,w [nring, jmax] (storage order) and the
+    per-ring scalars."""
+    jmax = p.jmax
+    n = p.imax * p.kmax
+    rb = 72 * jmax + 96
+    raw = np.frombuffer(buf, dtype=np.uint8)
+    assert raw.size == rb * n
+    rec = raw.reshape(n, rb)
+    f = rec[:, :40 * jmax].copy().view(np.float64).reshape(n, 5, jmax)
+    tail = rec[:, 72 * jmax + 32:].copy()
+    zs = tail[:, :32].view(np.float64)
+    ik = tail[:, 32:40].view(np.int32)
+    rot = tail[:, 40:56].view(np.float64)
+    rj = tail[:, 56:64].view(np.int32)
+    xs = rec[:, 40 * jmax:40 * jmax + 32].copy().view(np.float64)
+    return dict(r=f[:, 0], p=f[:, 1], u=f[:, 2], v=f[:, 3], w=f[:, 4], x=xs[:, 0], dx=xs[:, 1],
+                xvol=xs[:, 2], xc=xs[:, 3], z=zs[:, 0], dz=zs[:, 1], zvol=zs[:, 2], zc=zs[:, 3],
+                i=ik[:, 0], k=ik[:, 1], rot_v=rot[:, 0], res_v=rot[:, 1], rot_j=rj[:, 0], inc_j=rj[:, 1])
+
+
+def to_physical(a: np.ndarray, rot_j: np.ndarray) -> np.ndarray:
+    """Storage order -> physical azimuth order (j_phys = j_store + rot_j)."""
+    out = np.empty_like(a)
+    for m in range(a.shape[0]):
+        out[m] = np.roll(a[m], int(rot_j[m]))
+    return out
+
+
+@dataclass
+class Planet:
+    """struct body (variable_types.h:26-37)."""
+    m: float = 0.0
+    x: float = 0.0
+    y: float = 0.0
+    vx: float = 0.0
+    vy: float = 0.0
+    fx: float = 0.0
+    fy: float = 0.0
+    rs: float = 0.0
+
+    def to_c(self) -> pg_body:
+        return pg_body(self.m, self.x, self.y, self.vx, self.vy, self.fx, self.fy, self.rs)
+
+    def set_from(self, b: pg_body):
+        for k in ("m", "x", "y", "vx", "vy", "fx", "fy", "rs"):
+            setattr(self, k, getattr(b, k))
+
+
+class Run:
+    """One disk run resident on one GPU (pg_run)."""
+
+    def __init__(self, p: pg_params, device: int = 0):
+        self.p = p
+        self._h = None
+        h = C.c_void_p()
+        _check(_lib.lib().pg_create(C.byref(p), device, C.byref(h)), what="pg_create")
+        self._h = h
+
+    def close(self):
+        if self._h:
+            _lib.lib().pg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- state I/O (copy_bfile / save_cells) ----
+    def load(self, buf) -> "Run":
+        n = len(buf)
+        if isinstance(buf, (bytes, bytearray)):
+            cbuf = (C.c_char * n).from_buffer_copy(buf)
+        else:
+            cbuf = buf
+        _check(_lib.lib().pg_load_rings(self._h, cbuf, n), self, "pg_load_rings")
+        return self
+
+    def load_dump(self, path: str) -> "Run":
+        _check(_lib.lib().pg_load_dump(self._h, path.encode()), self, "pg_load_dump")
+        return self
+
+    def save(self) -> bytearray:
+        n = ring_bytes(self.p.jmax) * self.p.imax * self.p.kmax
+        buf = bytearray(n)
+        cbuf = (C.c_char * n).from_buffer(buf)
+        _check(_lib.lib().pg_save_rings(self._h, cbuf, n), self, "pg_save_rings")
+        return buf
+
+    def save_dump(self, path: str):
+        _check(_lib.lib().pg_save_dump(self._h, path.encode()), self, "pg_save_dump")
+
+    def sync(self):
+        _check(_lib.lib().pg_sync(self._h), self, "pg_sync")
+
+    def launches(self) -> int:
+        return _lib.lib().pg_launch_count(self._h)
+
+    # ---- fused device-resident loop ----
+    def clock_reset(self, startat: int = 0):
+        _check(_lib.lib().pg_clock_reset(self._h, startat), self, "pg_clock_reset")
+
+    def advance(self, nsteps: int, graph_chunk: int = 0) -> int:
+        taken = C.c_int(0)
+        if graph_chunk > 0:
+            st = _lib.lib().pg_advance_graph(self._h, nsteps, graph_chunk, C.byref(taken))
+        else:
+            st = _lib.lib().pg_advance(self._h, nsteps, C.byref(taken))
+        _check(st, self, "pg_advance")
+        return taken.value
+
+    def clock(self) -> tuple[pg_clock, Planet]:
+        c, b = pg_clock(), pg_body()
+        _check(_lib.lib().pg_clock_get(self._h, C.byref(c), C.byref(b)), self, "pg_clock_get")
+        pl = Planet()
+        pl.set_from(b)
+        return c, pl
+
+    def history(self, max_rows: int = 4096) -> np.ndarray:
+        buf = (C.c_double * (max_rows * HIST_COLS))()
+        n = C.c_int(0)
+        _check(_lib.lib().pg_history(self._h, buf, max_rows, C.byref(n)), self, "pg_history")
+        return np.frombuffer(buf, dtype=np.float64)[: n.value * HIST_COLS].reshape(n.value, HIST_COLS).copy()
+
+    # ---- host-driven loop with the reference's call sequence ----
+    def kernel_loop(self, nsteps: int, startat: int = 0, damping: bool = True, record=None):
+        """main.cu:270-441 restart path, host-driven: one get_dt (host sync),
+        Index_Shift, kick, bundle_sweep2D, damping, drift/forces/kick per step.
+        record(step, simtime, dt_used, planet, FrRot) is called after each step."""
+        p = self.p
+        dt = p.endtime
+        simtime = p.tmovie * startat
+        timem = 0.0
+        old_dt = 0.0
+        planet, FrRot = init_planet(p)
+        planet_forces(planet, FrRot, self, simtime)
+        make_pict = False
+        cont = True
+        ncycle = 0
+        s = 0
+        while s < nsteps and cont:
+            dt = get_dt(dt, self, FrRot)
+            if ncycle == p.ncycend:
+                cont = False
+            if simtime + dt >= p.endtime:
+                old_dt = dt
+                dt = p.endtime - simtime
+                make_pict = True
+                cont = False
+            if timem + dt >= p.tmovie:
+                old_dt = dt
+                dt = p.tmovie - timem
+                make_pict = True
+            dt_used = dt
+            Index_Shift(self, dt, FrRot)
+            if p.plnt_flag > 0:
+                FrRot = kick_drift_kick(p, planet, FrRot, 0.5 * dt, True)
+            if p.ndim == 2:
+                bundle_sweep2D(self, dt, planet, FrRot)
+            else:
+                bundle_sweep3D(self, dt, planet, FrRot)
+            if damping:
+                _check(_lib.lib().pg_damp(self._h, dt), self, "pg_damp")
+            simtime += dt
+            timem += dt
+            ncycle += 1
+            if p.plnt_flag > 0:
+                FrRot = kick_drift_kick(p, planet, FrRot, dt, False)
+                planet_forces(planet, FrRot, self, simtime)
+                FrRot = kick_drift_kick(p, planet, FrRot, 0.5 * dt, True)
+            if make_pict:
+                timem = 0.0
+                make_pict = False
+                dt = old_dt
+            if record is not None:
+                record(s, simtime, dt_used, planet, FrRot)
+            s += 1
+        return s, simtime, dt, planet, FrRot
+
+
+# ---- the reference's free functions ----------------------------------------------
+def get_dt(dt: float, run: Run, FrRot: float = 0.0) -> float:
+    out = C.c_double(0.0)
+    st = _lib.lib().pg_get_dt(run._h, dt, FrRot, C.byref(out))
+    if st not in (0, 4):   # PG_ERR_DT_COLLAPSE: the reference prints and goes on
+        _check(st, run, "pg_get_dt")
+    return out.value
+
+
+def Index_Shift(run: Run, dt: float, FrRot: float = 0.0):
+    _check(_lib.lib().pg_index_shift(run._h, dt, FrRot), run, "pg_index_shift")
+
+
+def bundle_sweep2D(run: Run, dt: float, planet: Planet, FrRot: float = 0.0):
+    b = planet.to_c()
+    _check(_lib.lib().pg_sweep2d(run._h, dt, C.byref(b), FrRot), run, "pg_sweep2d")
+
+
+def bundle_sweep3D(run: Run, dt: float, planet: Planet, FrRot: float = 0.0):
+    b = planet.to_c()
+    _check(_lib.lib().pg_sweep3d(run._h, dt, C.byref(b), FrRot), run, "pg_sweep3d")
+
+
+def GPU_output_reduction(run: Run, planet: Planet, exclude: float = 0.0, mode: int = 0) -> float:
+    b = planet.to_c()
+    out = C.c_double(0.0)
+    _check(_lib.lib().pg_reduce(run._h, C.byref(b), exclude, mode, C.byref(out)), run, "pg_reduce")
+    return out.value
+
+
+def init_planet(p: pg_params) -> tuple[Planet, float]:
+    b = pg_body()
+    fr = C.c_double(0.0)
+    _check(_lib.lib().pg_init_planet(C.byref(p), C.byref(b), C.byref(fr)), what="pg_init_planet")
+    pl = Planet()
+    pl.set_from(b)
+    return pl, fr.value
+
+
+def planet_forces(planet: Planet, FrRot: float, run: Run, simtime: float):
+    b = planet.to_c()
+    _check(_lib.lib().pg_planet_forces(run._h, C.byref(b), FrRot, simtime), run, "pg_planet_forces")
+    planet.set_from(b)
+
+
+def kick_drift_kick(p: pg_params, planet: Planet, FrRot: float, dt: float, kick: bool) -> float:
+    """Returns the new FrRot (the reference passes it by reference)."""
+    b = planet.to_c()
+    fr = C.c_double(FrRot)
+    _check(_lib.lib().pg_kick_drift_kick(C.byref(p), C.byref(b), C.byref(fr), dt, 1 if kick else 0),
+           what="pg_kick_drift_kick")
+    planet.set_from(b)
+    return fr.value
+
+
+def get_ecc(planet: Planet, FrRot: float) -> float:
+    b = planet.to_c()
+    return _lib.lib().pg_get_ecc(C.byref(b), FrRot)
+
+
+def torque_norm(p: pg_params) -> float:
+    """main.cu:421 normalisation of the mode-9 torque."""
+    return p.M_p * p.M_p * math.pow(p.R_p, 1.0 - p.p_alpha + (p.p_beta - 1.0)) / (p.sc_h * p.sc_h)

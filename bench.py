@@ -1,0 +1,345 @@
+"""Benchmark of the hydro step: zone-updates/s on one or more B200s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cfg0|cfg1|cfg2|big]
+
+A step is one full time step of the disk (get_dt, FARGO shift, planet kick,
+all directional sweeps, damping, drift/kick, diagnostics) over the whole
+grid, advanced by the device-resident loop (CUDA graphs of steps).  One
+zone-update = one cell advanced one step.  Synthetic data: the seeded disk of
+the chosen workload (no public dataset exists).  For N > 1 (torchrun, one
+rank per GPU) every rank advances its own independent disk (replicas; the
+path needs no exchange), and value = total zone-updates / max-over-ranks time.
+
+Timing: W untimed warm-up steps, then K timed steps between device
+synchronisations with CUDA events on the run's stream.  The 256x768 disk
+(4.7 MB) is L2 resident, so it is timed step by step with a 512 MB L2 flush
+between steps (outside the events); larger workloads exceed L2 and are timed
+as one region.
+
+roofline: the dominant kernel's algorithmic bytes (3 fields read + 3 written
+in FP64 = 48 B per cell per 2D sweep, 4 fields = 64 B in 3D) over its mean
+event-timed duration, against MEASURED_PEAKS.json's HBM copy bandwidth.
+e2e: the same metric through the reference-facing calls of the C ABI
+(pg_get_dt, pg_index_shift, pg_sweep2d, pg_damp, pg_reduce: host syncs as in
+main.cu), with the step's scalars (dt, planet, FrRot) going to the device
+and dt, mass and torque coming back every step.
+cpu_baseline: the CPU oracle (a restatement of the reference's sweeps in C,
+OpenMP over the box's cores) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (config index, overrides, description)
+    "cfg0": (0, {}, "2D r-phi disk 256x768 FP64, planet q=1e-3, FARGO, damping (configs[0])"),
+    "cfg1": (1, {}, "3D spherical disk 128x1024x32 FP64, reflecting midplane (configs[1])"),
+    "cfg2": (2, {}, "2D r-phi disk 1024x3072 FP64, same disk (configs[2] grid)"),
+    "big": (0, {"imax": 4096, "jmax": 12288}, "2D r-phi disk 4096x12288 FP64, same disk"),
+}
+
+
+def _peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._p = None
+        self._t = None
+
+    def start(self):
+        try:
+            self._p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._p = None
+            return
+
+        def rd():
+            for line in self._p.stdout:
+                self.rows.append([x.strip() for x in line.split(",")])
+        self._t = threading.Thread(target=rd, daemon=True)
+        self._t.start()
+
+    def stop(self) -> dict:
+        if self._p is not None:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except Exception:
+                self._p.kill()
+        if self._t is not None:
+            self._t.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        return dist, dist.get_rank(), ws
+    return None, 0, 1
+
+
+def _max_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_sample(p, steps: int, budget_s: float = 20.0):
+    """Time the CPU oracle on the same workload (bounded by budget_s)."""
+    import penguin_2_0_b200 as pg
+    from oracle.pyoracle import Oracle
+    orc = Oracle(p, pg.build_ic(p))
+    t0 = time.perf_counter()
+    orc.run_steps(1)   # first step includes set-up effects
+    one = time.perf_counter() - t0
+    n = max(1, min(steps, int(budget_s / max(one, 1e-6))))
+    orc2 = Oracle(p, pg.build_ic(p))
+    t0 = time.perf_counter()
+    done = orc2.run_steps(n).shape[0]
+    dt = time.perf_counter() - t0
+    cells = p.imax * p.jmax * p.kmax
+    return cells * done / dt, done, Oracle.threads(), dt
+
+
+def run_reference(args):
+    """--impl reference: the reference's sweeps restated in C (the reference
+    itself only exists as CUDA), on the host cores, same workload and metric."""
+    dist, rank, ws = _dist()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    import penguin_2_0_b200 as pg
+    from oracle.pyoracle import Oracle
+    which, over, desc = WORKLOADS[args.workload]
+    p = pg.params(which, **over)
+    p.nprin = 1
+    cells = p.imax * p.jmax * p.kmax
+    orc = Oracle(p, pg.build_ic(p))
+    if args.warmup:
+        orc.run_steps(min(args.warmup, 3))
+    budget = float(os.environ.get("PG_REF_BUDGET_S", "60"))
+    t0 = time.perf_counter()
+    orc2 = Oracle(p, pg.build_ic(p))
+    h = orc2.run_steps(1)
+    one = time.perf_counter() - t0
+    k = max(1, min(args.steps, int(budget / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    orc3 = Oracle(p, pg.build_ic(p))
+    done = orc3.run_steps(k).shape[0]
+    el = time.perf_counter() - t0
+    v = cells * done / el
+    line = {
+        "impl": "reference", "metric": "zone-updates/s", "value": v, "unit": "zone-updates/s",
+        "n_gpus": args.gpus, "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / done,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic seeded disk (no public dataset)",
+        "config": {"workload": desc, "cells": cells, "sample": f"{done} steps of {k} requested"},
+        "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": Oracle.threads(), "kind": "port",
+                         "sample": f"{done} full steps of the {args.workload} disk"},
+        "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's hot path exists only as CUDA; this arm runs its restatement (oracle/pg_oracle.c) "
+                "with OpenMP on the host cores",
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg0", choices=list(WORKLOADS))
+    ap.add_argument("--chunk", type=int, default=50, help="steps per CUDA graph")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    dist, rank, ws = _dist()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    import penguin_2_0_b200 as pg
+
+    which, over, desc = WORKLOADS[args.workload]
+    p = pg.params(which, **over)
+    p.nprin = 100
+    p.seed = rank
+    p.endtime = 1.0e9
+    p.tmovie = 1.0e9
+    cells = p.imax * p.jmax * p.kmax
+    ic = pg.build_ic(p)
+    run = pg.Run(p, local).load(ic)
+    run.clock_reset(0)
+    l2_resident = args.workload == "cfg0"
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") if l2_resident else None
+
+    # warm-up (builds the step graph too)
+    run.advance(args.warmup, graph_chunk=1 if l2_resident else args.chunk)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = run.launches()
+    run.timing(True)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    if l2_resident:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            run.advance(1, graph_chunk=1)
+        ms, cnt = run.timing_read()
+        total_ms = ms[3]
+    else:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        s = torch.cuda.ExternalStream(run.stream_ptr())
+        ev0.record(s)
+        run.advance(args.steps, graph_chunk=args.chunk)
+        ev1.record(s)
+        ev1.synchronize()
+        total_ms = ev0.elapsed_time(ev1)
+        run.timing(False)
+        ms, cnt = run.timing_read()
+    torch.cuda.synchronize()
+    _barrier(dist)
+    launches = run.launches() - l0
+    clk = clocks.stop()
+    run.timing(False)
+    c, _ = run.clock()
+    assert c.ncycle == args.warmup + args.steps, (c.ncycle, args.warmup, args.steps)
+    t_max = _max_over_ranks(dist, total_ms)
+    value = cells * args.steps * ws / (t_max / 1e3)
+
+    # per-kernel timing (separate short pass, event pairs around each sweep)
+    run.timing(True)
+    nk = 20
+    if l2_resident:
+        for _ in range(nk):
+            flush.zero_()
+            torch.cuda.synchronize()
+            run.advance(1)
+    else:
+        run.advance(nk)
+    kms, kcnt = run.timing_read()
+    run.timing(False)
+    kinds = ["sweep_x", "sweep_y", "sweep_z"]
+    mean = {kinds[i]: kms[i] / kcnt[i] for i in range(3) if kcnt[i]}
+    top = max(mean, key=mean.get)
+    nfield = 4 if p.ndim == 3 else 3
+    bytes_per_launch = 2 * nfield * 8 * cells
+    peak, peak_kind = _peaks()
+    achieved = bytes_per_launch / (mean[top] / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"{top}_{args.workload}.md")
+    if os.path.exists(prof):
+        for line in open(prof):
+            if line.startswith("traffic_bytes_per_launch:"):
+                traffic = float(line.split(":")[1])
+
+    # e2e through the reference-facing calls (host-driven loop, host syncs)
+    e2e_steps = max(3, min(args.steps // 10, 200))
+    run2 = pg.Run(p, local).load(ic)
+    run2.kernel_loop(2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+
+    def rec(s, simtime, dt_used, planet, FrRot):
+        pg.GPU_output_reduction(run2, planet, 0.0, 0)
+        if p.plnt_flag:
+            pg.GPU_output_reduction(run2, planet, 0.0, 9)
+
+    run2.kernel_loop(e2e_steps, record=rec)
+    torch.cuda.synchronize()
+    e2e_el = _max_over_ranks(dist, time.perf_counter() - t0)
+    e2e_value = cells * e2e_steps * ws / e2e_el
+    run2.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        v, done, cores, el = cpu_sample(p, 400, budget_s=float(os.environ.get("PG_CPU_BUDGET_S", "15")))
+        cpu = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "port",
+               "sample": f"{done} steps of the same disk in {el:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic seeded disk (no public dataset), one independent disk per GPU",
+            "config": {"workload": desc, "cells": cells, "imax": p.imax, "jmax": p.jmax, "kmax": p.kmax,
+                       "parallelism": f"replicas{ws}",
+                       "l2": "flushed between steps (512 MB write)" if l2_resident
+                       else "working set larger than L2, CUDA graphs of %d steps" % args.chunk},
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak,
+                         "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "bytes_per_launch": bytes_per_launch,
+                         "mean_launch_ms": mean[top], "kernels_ms": mean},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": 64 + 16,
+                    "d2h_bytes_per_step": 8 + 8 + 8,
+                    "path": "host loop over pg_get_dt/pg_index_shift/pg_sweep2d/pg_damp/pg_reduce"},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    run.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -120,6 +120,18 @@ int pg_build_ic(const pg_params *p, void *rings, size_t bytes);
 /* Run label of create_label() (output.cu:57-88) into buf.                  */
 int pg_label(const pg_params *p, char *buf, size_t len);
 
+/* "<dir>/binary_<label>_<NNNNN>": the dump name of main.cu:124 with
+ * frame_num() zero padding (global.cu:27-38).                              */
+int pg_dump_name(const pg_params *p, const char *dir, int frame, char *buf, size_t len);
+
+/* files/time_<label>.dat rows (main.cu:417-427): simtime, mass, normalised
+ * torque, planet x y vx vy fx fy, eccentricity, semi-major axis; 11 doubles
+ * per row written with 16 significant digits, space separated.             */
+int pg_write_time_rows(const char *path, const double *rows, int nrows, int append);
+
+/* read/para_<label>.dat of write_para_file (output.cu:90-109).              */
+int pg_write_para_file(const pg_params *p, const char *path, const char *mainp);
+
 /* ---- run lifetime -------------------------------------------------------- */
 
 /* Replaces the allocation block of main.cu:141-219.  Device memory is owned
@@ -208,8 +220,17 @@ typedef struct pg_device_view {
 } pg_device_view;
 int pg_device_view_get(pg_run *run, pg_device_view *view);
 
-/* Count of kernel launches issued by this run since creation.             */
+/* Count of kernel launches issued by this run since creation (kernels inside
+ * a replayed CUDA graph count once per replay).                             */
 int64_t pg_launch_count(const pg_run *run);
+
+/* Kernel timing with CUDA events on the run's stream.  While enabled, every
+ * step enqueued by pg_advance / pg_advance_graph records event pairs around
+ * its radial (kind 0), azimuthal (1) and polar (2) sweeps and around the
+ * whole step (3).  pg_timing_read synchronises, returns per kind the summed
+ * milliseconds and the number of timed launches, and clears the record.    */
+int pg_timing(pg_run *run, int on);
+int pg_timing_read(pg_run *run, double *ms_sum, int64_t *counts, int nkinds);
 
 #ifdef __cplusplus
 }

@@ -105,6 +105,9 @@ def lib() -> C.CDLL:
         "pg_write_ic": (C.c_int, [P, C.c_char_p]),
         "pg_build_ic": (C.c_int, [P, vp, C.c_size_t]),
         "pg_label": (C.c_int, [P, C.c_char_p, C.c_size_t]),
+        "pg_dump_name": (C.c_int, [P, C.c_char_p, C.c_int, C.c_char_p, C.c_size_t]),
+        "pg_write_time_rows": (C.c_int, [C.c_char_p, dp, C.c_int, C.c_int]),
+        "pg_write_para_file": (C.c_int, [P, C.c_char_p, C.c_char_p]),
         "pg_create": (C.c_int, [P, C.c_int, C.POINTER(vp)]),
         "pg_destroy": (C.c_int, [vp]),
         "pg_last_error": (C.c_char_p, [vp]),
@@ -132,6 +135,8 @@ def lib() -> C.CDLL:
         "pg_history": (C.c_int, [vp, dp, C.c_int, ip]),
         "pg_device_view_get": (C.c_int, [vp, C.POINTER(pg_device_view)]),
         "pg_launch_count": (C.c_int64, [vp]),
+        "pg_timing": (C.c_int, [vp, C.c_int]),
+        "pg_timing_read": (C.c_int, [vp, dp, C.POINTER(C.c_int64), C.c_int]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name, None)

@@ -284,6 +284,9 @@ int check_params(const pg_params *p, std::string &why) {
   if (p->ndim == 3 && !(p->ngeomx == 2 && p->ngeomy == 4 && p->ngeomz == 5)) {
     why = "3D needs spherical geometry (ngeomx=2, ngeomy=4, ngeomz=5)"; return PG_ERR_PARAMS;
   }
+  if (p->ndim == 3 && p->kmax < 2 * 3) {
+    why = "3D needs kmax >= 6 (the reflecting midplane mirrors 6 layers)"; return PG_ERR_PARAMS;
+  }
   if (p->ndim == 3 && !(p->nudr == 3 && (p->ntop == 0 || p->ntop == 3))) {
     why = "3D needs fixed lower theta layers (nudr=3) and a fixed or reflecting top (ntop 3 or 0)"; return PG_ERR_PARAMS;
   }
@@ -442,6 +445,41 @@ int pg_write_ic(const pg_params *p, const char *path) {
   size_t w = std::fwrite(buf.data(), 1, bytes, f);
   std::fclose(f);
   return (w == bytes) ? PG_OK : PG_ERR_IO;
+}
+
+int pg_dump_name(const pg_params *p, const char *dir, int frame, char *buf, size_t len) {
+  if (!p || !dir || !buf || frame < 0 || frame > 99999) return PG_ERR_ARG;
+  char num[8];
+  std::snprintf(num, sizeof num, "%05d", frame);
+  std::string s = std::string(dir) + "/binary_" + pg::label(*p) + "_" + num;
+  if (s.size() + 1 > len) return PG_ERR_ARG;
+  std::memcpy(buf, s.c_str(), s.size() + 1);
+  return PG_OK;
+}
+
+int pg_write_time_rows(const char *path, const double *rows, int nrows, int append) {
+  if (!path || (!rows && nrows > 0) || nrows < 0) return PG_ERR_ARG;
+  FILE *f = std::fopen(path, append ? "a" : "w");
+  if (!f) return PG_ERR_IO;
+  for (int r = 0; r < nrows; r++) {
+    const double *q = rows + 11 * (size_t)r;
+    for (int c = 0; c < 11; c++) std::fprintf(f, c ? " %.16g" : "%.16g", q[c]);
+    std::fputc('\n', f);
+  }
+  return std::fclose(f) == 0 ? PG_OK : PG_ERR_IO;
+}
+
+int pg_write_para_file(const pg_params *p, const char *path, const char *mainp) {
+  if (!p || !path || !mainp) return PG_ERR_ARG;
+  FILE *f = std::fopen(path, "w");
+  if (!f) return PG_ERR_IO;
+  // ofstream with precision(16): %.16g
+  std::fprintf(f, "%d\n%d\n%d\n%d\n", p->imax, p->jmax, p->kmax, 1);
+  std::fprintf(f, "%.16g\n%.16g\n%.16g\n", p->gam, p->sc_h, p->tmovie);
+  std::fprintf(f, "%s\n%s\n", mainp, pg::label(*p).c_str());
+  std::fprintf(f, "%d\n%d\n%d\n", p->grspx, p->grspy, p->grspz);
+  std::fprintf(f, "%.16g %.16g\n%.16g %.16g\n%.16g %.16g\n", p->xmin, p->xmax, p->ymin, p->ymax, p->zmin, p->zmax);
+  return std::fclose(f) == 0 ? PG_OK : PG_ERR_IO;
 }
 
 int pg_label(const pg_params *p, char *buf, size_t len) {

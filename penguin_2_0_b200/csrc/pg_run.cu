@@ -59,7 +59,31 @@ struct pg_run {
   // captured step graphs
   cudaGraphExec_t gexec = nullptr;
   int gsteps = 0;
+  int64_t graph_kernels = 0;       // kernels per replay of gexec
+  // event timing
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_next = 0;
+  struct Mark { int kind; size_t a, b; };
+  std::vector<Mark> marks;
 };
+
+static int ev_pair(pg_run *run, int kind, size_t &a) {
+  // reserve two events; record the first now
+  while (run->ev_pool.size() < run->ev_next + 2) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return PG_ERR_CUDA;
+    run->ev_pool.push_back(e);
+  }
+  a = run->ev_next;
+  run->ev_next += 2;
+  if (cudaEventRecord(run->ev_pool[a], run->stream) != cudaSuccess) return PG_ERR_CUDA;
+  run->marks.push_back({kind, a, a + 1});
+  return PG_OK;
+}
+static int ev_close(pg_run *run, size_t a) {
+  return cudaEventRecord(run->ev_pool[a + 1], run->stream) == cudaSuccess ? PG_OK : PG_ERR_CUDA;
+}
 
 #define CK(call)                                                                   \
   do {                                                                             \
@@ -172,6 +196,7 @@ int pg_destroy(pg_run *run) {
   cudaSetDevice(run->dev);
   if (run->stream) cudaStreamSynchronize(run->stream);
   if (run->gexec) cudaGraphExecDestroy(run->gexec);
+  for (auto e : run->ev_pool) cudaEventDestroy(e);
   for (auto &b : run->planes)
     for (auto &f : b) if (f) cudaFree(f);
   cudaFree(run->p0);
@@ -673,15 +698,26 @@ static int enqueue_step(pg_run *run, bool first_p0) {
   c.fuse = 0;
   int a = run->cur;
   int n = 0;
+  const bool tm = run->timing;
+  size_t e_step = 0, e_k = 0;
+  if (tm && ev_pair(run, 3, e_step)) return fail(run, PG_ERR_CUDA, "event record");
   pgk::prestep(run->clk, run->T, P.FARGO_flag, s); n++;
+  if (tm && ev_pair(run, 0, e_k)) return fail(run, PG_ERR_CUDA, "event record");
   pgk::sweep_x(run->T, planes_fwd(run, a, first_p0 ? run->p0 : nullptr), run->ph, c, P.ndim, s); n++;
+  if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
   if (P.ndim == 2) {
     c.fuse = 1;
+    if (tm && ev_pair(run, 1, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 2, s); n++;
+    if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
   } else {
+    if (tm && ev_pair(run, 1, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 3, s); n++;
+    if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     // 3D: damping and CFL after the polar sweep
+    if (tm && ev_pair(run, 2, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, P.ntop, s); n++;
+    if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     double **cp = run->planes[1 - a];
     pgk::damp_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->clk, s); n++;
     pgk::cfl_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->ph, run->clk, s); n++;
@@ -698,6 +734,7 @@ static int enqueue_step(pg_run *run, bool first_p0) {
     }
     pgk::record(run->clk, s); n++;
   }
+  if (tm && ev_close(run, e_step)) return fail(run, PG_ERR_CUDA, "event record");
   return check_launch(run, n);
 }
 
@@ -752,22 +789,31 @@ int pg_advance_graph(pg_run *run, int nsteps, int chunk, int *taken) {
   if (!run->gexec || run->gsteps != chunk) {
     if (run->gexec) { cudaGraphExecDestroy(run->gexec); run->gexec = nullptr; }
     int cur0 = run->cur;
+    bool tm = run->timing;
+    run->timing = false;
+    int64_t l0 = run->launches;
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(run->stream, cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < chunk; i++) {
       int e = enqueue_step(run, false);
-      if (e) { cudaStreamEndCapture(run->stream, &g); return e; }
+      if (e) { cudaStreamEndCapture(run->stream, &g); run->timing = tm; return e; }
     }
     CK(cudaStreamEndCapture(run->stream, &g));
+    run->timing = tm;
     CK(cudaGraphInstantiate(&run->gexec, g, 0));
     cudaGraphDestroy(g);
     run->gsteps = chunk;
+    run->graph_kernels = run->launches - l0;
+    run->launches = l0;
     run->cur = cur0;
-    run->launches -= 0;
   }
   int64_t per = 0;
   for (; done + chunk <= nsteps; done += chunk) {
+    size_t e = 0;
+    if (run->timing && ev_pair(run, 3, e)) return fail(run, PG_ERR_CUDA, "event record");
     CK(cudaGraphLaunch(run->gexec, run->stream));
+    if (run->timing && ev_close(run, e)) return fail(run, PG_ERR_CUDA, "event record");
+    run->launches += run->graph_kernels;
     per++;
   }
   for (; done < nsteps; done++) {
@@ -775,6 +821,29 @@ int pg_advance_graph(pg_run *run, int nsteps, int chunk, int *taken) {
   }
   (void)per;
   return finish_advance(run, before, taken);
+}
+
+int pg_timing(pg_run *run, int on) {
+  if (!run) return PG_ERR_ARG;
+  run->timing = on != 0;
+  return PG_OK;
+}
+
+int pg_timing_read(pg_run *run, double *ms_sum, int64_t *counts, int nkinds) {
+  if (!run || !ms_sum || !counts) return PG_ERR_ARG;
+  CK(cudaSetDevice(run->dev));
+  CK(cudaStreamSynchronize(run->stream));
+  for (int k = 0; k < nkinds; k++) { ms_sum[k] = 0.0; counts[k] = 0; }
+  for (const auto &m : run->marks) {
+    if (m.kind < 0 || m.kind >= nkinds) continue;
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, run->ev_pool[m.a], run->ev_pool[m.b]));
+    ms_sum[m.kind] += ms;
+    counts[m.kind] += 1;
+  }
+  run->marks.clear();
+  run->ev_next = 0;
+  return PG_OK;
 }
 
 int pg_history(pg_run *run, double *rows, int max, int *rows_out) {

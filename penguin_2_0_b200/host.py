@@ -192,6 +192,20 @@ class Run:
     def launches(self) -> int:
         return _lib.lib().pg_launch_count(self._h)
 
+    def timing(self, on: bool):
+        _check(_lib.lib().pg_timing(self._h, 1 if on else 0), self, "pg_timing")
+
+    def timing_read(self) -> tuple[list, list]:
+        ms = (C.c_double * 4)()
+        cnt = (C.c_int64 * 4)()
+        _check(_lib.lib().pg_timing_read(self._h, ms, cnt, 4), self, "pg_timing_read")
+        return list(ms), list(cnt)
+
+    def stream_ptr(self) -> int:
+        v = _lib.pg_device_view()
+        _check(_lib.lib().pg_device_view_get(self._h, C.byref(v)), self, "pg_device_view_get")
+        return v.stream or 0
+
     # ---- fused device-resident loop ----
     def clock_reset(self, startat: int = 0):
         _check(_lib.lib().pg_clock_reset(self._h, startat), self, "pg_clock_reset")

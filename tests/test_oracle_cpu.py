@@ -1,0 +1,48 @@
+"""The CPU oracle on its own: determinism, conservation structure and the
+reference behaviours it restates (chunk-edge viscosity, idle last chunk)."""
+import numpy as np
+
+import penguin_2_0_b200 as pg
+from oracle.pyoracle import Oracle
+
+
+def _run(p, n):
+    o = Oracle(p, pg.build_ic(p))
+    h = o.run_steps(n)
+    return h, pg.dump_fields(o.save(), p)
+
+
+def test_oracle_deterministic_and_finite():
+    p = pg.params(0, imax=128, jmax=132)
+    h1, f1 = _run(p, 3)
+    h2, f2 = _run(p, 3)
+    np.testing.assert_array_equal(h1, h2)
+    for k in ("r", "u", "v"):
+        np.testing.assert_array_equal(f1[k], f2[k])
+        assert np.all(np.isfinite(f1[k]))
+    assert np.all(f1["r"] > 0)
+
+
+def test_unperturbed_disk_without_planet_stays_near_equilibrium():
+    # no planet, no noise: the pressure-supported disk is close to steady
+    p = pg.params(0, imax=128, jmax=132, plnt_flag=0, noise_amp=0.0, kill_rin=0.0, kill_rout=0.0)
+    h, f = _run(p, 5)
+    ic = pg.dump_fields(pg.build_ic(p), p)
+    inner = slice(8, 120)
+    rel = np.max(np.abs(f["r"][inner] / ic["r"][inner] - 1.0))
+    assert rel < 1e-5, rel
+    # axisymmetry is kept to rounding
+    assert np.max(np.std(f["r"][inner], axis=1) / np.mean(f["r"][inner], axis=1)) < 1e-12
+
+
+def test_idle_last_radial_chunk_is_reproduced():
+    # imax % 116 == 0: ppm.cu:48 gives the last chunk lim = 12, so rings
+    # 116..231 are never touched by the radial sweep; with no planet, no
+    # viscosity and no noise the azimuthal sweep leaves an axisymmetric ring
+    # unchanged too, so those rings keep their initial values.
+    p = pg.params(0, imax=232, jmax=240, plnt_flag=0, noise_amp=0.0, kill_rin=0.0, kill_rout=0.0,
+                  visc_flag=0, FARGO_flag=0)
+    ic = pg.dump_fields(pg.build_ic(p), p)
+    h, f = _run(p, 1)
+    assert np.array_equal(f["u"][116:], ic["u"][116:])
+    assert not np.array_equal(f["u"][:116], ic["u"][:116])

@@ -47,6 +47,7 @@ WORKLOADS = {
     "cfg1": (1, {}, "3D spherical disk 128x1024x32 FP64, reflecting midplane (configs[1])"),
     "cfg2": (2, {}, "2D r-phi disk 1024x3072 FP64, same disk (configs[2] grid)"),
     "big": (0, {"imax": 4096, "jmax": 12288}, "2D r-phi disk 4096x12288 FP64, same disk"),
+    "prof": (0, {"imax": 2048, "jmax": 6144}, "2D r-phi disk 2048x6144 FP64 (profiling case, > L2)"),
 }
 
 
@@ -201,6 +202,8 @@ def main():
     ap.add_argument("--workload", default="cfg0", choices=list(WORKLOADS))
     ap.add_argument("--chunk", type=int, default=50, help="steps per CUDA graph")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--profile", action="store_true",
+                    help="only W + K steps of the fused loop (stream launches), no extra legs; for ncu")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -223,6 +226,14 @@ def main():
     ic = pg.build_ic(p)
     run = pg.Run(p, local).load(ic)
     run.clock_reset(0)
+    if args.profile:
+        run.advance(args.warmup)
+        run.advance(args.steps)
+        torch.cuda.synchronize()
+        c, _ = run.clock()
+        print(json.dumps({"profile": args.workload, "steps": int(c.ncycle), "status": int(c.status)}))
+        run.close()
+        return
     l2_resident = args.workload == "cfg0"
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") if l2_resident else None
 

@@ -16,7 +16,8 @@
 //     (mode 9, normalised as main.cu:421) and, after the listed steps, the
 //     full rings in the dump layout.
 //
-// usage: penguin_ref <ic_dump> <nsteps> <outdir> <steps-to-save, comma separated>
+// usage: penguin_ref <ic_dump> <nsteps> <outdir> <steps-to-save, comma separated> [nodiag]
+// (nodiag: skip the mass/torque reductions, for timing the sweeps)
 #include <unistd.h>
 #include <cstdio>
 #include <cstdlib>
@@ -75,6 +76,7 @@ int main(int argc, char **argv)
     return 2;
   }
   const char *icpath = argv[1];
+  bool diag = !(argc > 5 && std::string(argv[5]) == "nodiag");
   int nsteps = atoi(argv[2]);
   string outdir = argv[3];
   bool keep[100000] = {false};
@@ -187,11 +189,13 @@ int main(int argc, char **argv)
     kick_drift_kick(planet, FrRot, set, simtime, 0.5 * dt, true);
     #endif
     if (make_pict) { timem = 0.0; make_pict = false; dt = old_dt; }
-    sdp mass = GPU_output_reduction(set, planet, 0.0);
-    sdp torque = 0.0;
-    #if plnt_flag > 0
-    torque = GPU_output_reduction(set, planet, 0.0, 9) / (M_p * M_p * pow(R_p, 1.0 - p_alpha + (p_beta - 1.0)) / (sc_h * sc_h));
-    #endif
+    sdp mass = 0.0, torque = 0.0;
+    if (diag) {
+      mass = GPU_output_reduction(set, planet, 0.0);
+      #if plnt_flag > 0
+      torque = GPU_output_reduction(set, planet, 0.0, 9) / (M_p * M_p * pow(R_p, 1.0 - p_alpha + (p_beta - 1.0)) / (sc_h * sc_h));
+      #endif
+    }
     fprintf(hf, "%d %a %a %a %a %a %a\n", s, simtime, dt_used, mass, torque, FrRot, planet.y);
     if (s + 1 < 100000 && keep[s + 1]) {
       CudaSafeCall(cudaMemcpy(set[0].h_rings, set[0].rings, set[0].memsize, cudaMemcpyDeviceToHost));

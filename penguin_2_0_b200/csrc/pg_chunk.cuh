@@ -291,9 +291,11 @@ __device__ __forceinline__ void ppm_chunk(ChunkShm &S, int n, int nmax, double d
       fld[n] = (fld[n] * mm + fl) * invm;
     }
   };
+  // 2D slots that stay exactly zero are skipped: w in the radial sweep,
+  // v (= w) in the azimuthal one, whose w slot carries v_r
   remap_field(S.u);
-  remap_field(S.v);
-  if (THREED) remap_field(S.w);
+  if (AXIS != 1 || THREED) remap_field(S.v);
+  if (AXIS == 1 || THREED) remap_field(S.w);
   __syncthreads();
 }
 

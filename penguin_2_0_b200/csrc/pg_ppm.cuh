@@ -15,8 +15,9 @@
 //    the same Jacobi update);
 //  * the q = p/rho remap (remap.cu:291-300) is skipped: in EOS 0 the sweep
 //    store overwrites p with rho*cs2 (ppm.cu:139);
-//  * in 2D the w remap is skipped (w stays exactly 0) and umid *= pmid
-//    (evolve.cu:73, used by EOS 2 only) is dropped;
+//  * in 2D the remap of the slot holding w is skipped (w stays exactly 0:
+//    the w slot of the radial sweep, the v slot of the azimuthal sweep) and
+//    umid *= pmid (evolve.cu:73, used by EOS 2 only) is dropped;
 //  * cs2(r) and nu(r) come from per-ring tables computed on the device with
 //    the same expressions.
 #pragma once

@@ -69,3 +69,28 @@ class OracleLoop:
 
     def fields(self):
         return pg.dump_fields(self.o.save(), self.p)
+
+
+def torque_abs_scale(fields, p, planet):
+    """Sum over cells of |integrand| of the mode-9 torque (device_func.cu:96-108),
+    normalised like main.cu:421: the scale that bounds the rounding of a sum
+    whose terms cancel."""
+    rot = fields["rot_j"]
+    r = to_phys(fields["r"], rot)
+    xc = fields["xc"][:, None]
+    jmax = p.jmax
+    dy = 2 * np.pi / jmax
+    phi = (np.arange(jmax) + 0.5) * dy
+    cosf = np.cos(phi - planet.y)[None, :]
+    sinf = np.sin(phi - planet.y)[None, :]
+    Rp = np.sqrt(xc * xc + planet.x ** 2 - 2 * planet.x * xc * cosf + planet.rs ** 2)
+    g = -planet.m * planet.x * sinf / Rp ** 3 + planet.m * sinf / planet.x ** 2
+    integ = g * xc * (r - xc ** (-p.p_alpha)) * fields["xvol"][:, None] * dy
+    return float(np.sum(np.abs(integ))) / pg.torque_norm(p)
+
+
+def to_phys(a, rot):
+    out = np.empty_like(a)
+    for m in range(a.shape[0]):
+        out[m] = np.roll(a[m], int(rot[m]))
+    return out

@@ -19,6 +19,7 @@ import json
 import os
 import subprocess
 import sys
+import time
 
 import numpy as np
 
@@ -27,24 +28,41 @@ sys.path.insert(0, ROOT)
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 # name -> (base workload, overrides, nsteps, steps kept in the fixture)
+#
+# Every size keeps the last chunk of each pencil warp aligned: n % 116 is 0,
+# 20, 52 or 84, so the chunk's lim (n % 116 + 12) is 12 (all threads active),
+# 32, 64 or 96.  With any other remainder the reference's sweepx/sweepy
+# (ppm.cu:50-156, 198-303) leave a warp partially inside the
+# `if (i_ring < iblk+n_pad)` block that holds ~30 __syncthreads(): divergent
+# barriers inside a warp, undefined since independent thread scheduling; on
+# a B200 the 128x132 case (lim 24) never finished.
 CASES = {
-    # two radial chunks (128 = 116 + 12), two azimuthal chunks (132 = 116 + 16)
-    "g128x132": (0, dict(imax=128, jmax=132), 20, (1, 2, 5, 20)),
-    # the 256 x 768 disk itself; fixtures keep a strided subsample
-    "cfg0": (0, dict(), 12, (1, 12)),
+    # two radial chunks (136 = 116 + 20), two azimuthal chunks
+    "g136x136": (0, dict(imax=136, jmax=136), 12, (1, 2, 5, 12)),
+    # near the 256 x 768 disk: 252 = 2*116 + 20, 780 = 6*116 + 84
+    "g252x780": (0, dict(imax=252, jmax=780), 8, (1, 8)),
     # imax % 116 == 0: the last radial chunk is never updated (ppm.cu:48)
-    "g232x240": (0, dict(imax=232, jmax=240), 4, (1, 4)),
+    "g232x200": (0, dict(imax=232, jmax=200), 4, (1, 4)),
     # jmax % 116 == 0: the last azimuthal chunk is never updated (ppm.cu:196)
-    "g130x232": (0, dict(imax=130, jmax=232), 4, (1, 4)),
+    "g168x232": (0, dict(imax=168, jmax=232), 4, (1, 4)),
     # no planet, no viscosity, no flattening, no FARGO, no damping
-    "g120x150_plain": (0, dict(imax=120, jmax=150, plnt_flag=0, visc_flag=0, flat_flag=0,
+    "g136x200_plain": (0, dict(imax=136, jmax=200, plnt_flag=0, visc_flag=0, flat_flag=0,
                                FARGO_flag=0, kill_rin=0.0, kill_rout=0.0), 6, (1, 6)),
+}
+
+
+# Timing builds of the reference (sweeps only, no diagnostics reductions):
+# name -> (base workload, overrides, nsteps).  Warp-aligned sizes near the
+# 256x768 and 1024x3072 disks.
+PERF_CASES = {
+    "perf_g252x780": (0, dict(imax=252, jmax=780), 200),
+    "perf_g1012x3100": (0, dict(imax=1012, jmax=3100), 40),
 }
 
 
 def params_for(case):
     from penguin_2_0_b200 import _lib
-    base, over, *_ = CASES[case]
+    base, over, *_ = CASES[case] if case in CASES else PERF_CASES[case]
     p = _lib.pg_params()
     st = _lib.lib().pg_config_params(base, C.byref(p))
     assert st == 0
@@ -58,13 +76,38 @@ def to_json(p):
 
 
 def cmd_build():
-    for case in CASES:
+    for case in list(CASES) + list(PERF_CASES):
         p = params_for(case)
         d = os.path.join(ROOT, "oracle", "_ref", case)
         os.makedirs(d, exist_ok=True)
         pj = os.path.join(d, "params.json")
         json.dump(to_json(p), open(pj, "w"), indent=1)
-        subprocess.check_call([os.path.join(ROOT, "oracle", "ref", "build_ref.sh"), case, pj])
+        mode = "perf" if case in PERF_CASES else "golden"
+        subprocess.check_call([os.path.join(ROOT, "oracle", "ref", "build_ref.sh"), case, pj, mode])
+
+
+def cmd_perf(rawdir):
+    """Time the reference's bundle_sweep2D (CUDA events around it, summed by
+    the harness) on the perf builds; prints one JSON line per case."""
+    from penguin_2_0_b200 import _lib
+    L = _lib.lib()
+    for case, (_, _, nsteps) in PERF_CASES.items():
+        p = params_for(case)
+        p.nprin = 100
+        out = os.path.join(rawdir, case)
+        os.makedirs(out, exist_ok=True)
+        ic = os.path.join(out, "ic.bin")
+        assert L.pg_write_ic(C.byref(p), ic.encode()) == 0
+        exe = os.path.join(ROOT, "oracle", "_ref", case, "penguin_ref")
+        r = subprocess.run(["timeout", "-k", "10", "300", exe, ic, str(nsteps), out, "0", "nodiag"],
+                           capture_output=True, text=True)
+        os.remove(ic)
+        if r.returncode != 0:
+            raise SystemExit(f"{case}: reference exited {r.returncode}: {r.stderr[-400:]}")
+        d = json.loads(r.stdout.strip().splitlines()[-1])
+        cells = p.imax * p.jmax
+        d.update(case=case, zone_updates_per_s=cells * d["steps"] / (d["sweep_ms_total"] / 1e3))
+        print(json.dumps(d), flush=True)
 
 
 def cmd_run(rawdir):
@@ -77,13 +120,17 @@ def cmd_run(rawdir):
         ic = os.path.join(out, "ic.bin")
         assert L.pg_write_ic(C.byref(p), ic.encode()) == 0
         exe = os.path.join(ROOT, "oracle", "_ref", case, "penguin_ref")
-        r = subprocess.run([exe, ic, str(nsteps), out, ",".join(map(str, keep))],
-                           capture_output=True, text=True)
+        t0 = time.time()
+        try:
+            r = subprocess.run(["timeout", "-k", "10", "120", exe, ic, str(nsteps), out,
+                                ",".join(map(str, keep))], capture_output=True, text=True)
+        except Exception as e:  # pragma: no cover
+            raise SystemExit(f"{case}: {e}")
         open(os.path.join(out, "stdout.txt"), "w").write(r.stdout + r.stderr)
         if r.returncode != 0:
             raise SystemExit(f"{case}: reference exited {r.returncode}: {r.stderr[-400:]}")
         os.remove(ic)
-        print(case, r.stdout.strip())
+        print(case, f"{time.time() - t0:.1f}s", r.stdout.strip(), flush=True)
 
 
 def read_rings(path, p):
@@ -106,8 +153,8 @@ def cmd_pack(rawdir, outdir=HERE, full=None):
         hist = np.array([[float.fromhex(x) for x in r[1:]] for r in rows])
         out = {"hist": hist}
         stride = 1
-        if case == "cfg0":
-            stride = 7  # every 7th cell of the 196608 keeps the fixture small
+        if case == "g252x780":
+            stride = 7  # every 7th cell keeps the fixture small
         for s in keep:
             f, rot_j = read_rings(os.path.join(src, f"state_{s:05d}.bin"), p)
             sel = f[:, [0, 2, 3], :].reshape(f.shape[0], 3, -1)
@@ -119,9 +166,10 @@ def cmd_pack(rawdir, outdir=HERE, full=None):
             out[f"rot_j_{s}"] = rot_j
         out["stride"] = np.array(stride)
         np.savez_compressed(os.path.join(outdir, f"{case}.npz"), **out)
-        if full and case == "cfg0":
+        if full and case == "g252x780":
             f, rot_j = read_rings(os.path.join(src, f"state_{keep[0]:05d}.bin"), p)
-            np.savez_compressed(os.path.join(full, "cfg0_full_step1.npz"), fields=f[:, [0, 2, 3], :], rot_j=rot_j)
+            np.savez_compressed(os.path.join(full, "g252x780_full_step1.npz"), fields=f[:, [0, 2, 3], :],
+                                rot_j=rot_j)
         print("packed", case)
 
 
@@ -131,6 +179,8 @@ if __name__ == "__main__":
         cmd_build()
     elif what == "run":
         cmd_run(sys.argv[2])
+    elif what == "perf":
+        cmd_perf(sys.argv[2])
     elif what == "pack":
         cmd_pack(sys.argv[2], *(sys.argv[3:5]))
     else:

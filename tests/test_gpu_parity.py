@@ -1,22 +1,26 @@
 """CUDA path (through the C ABI) against the CPU oracle on the same seeded
-inputs, step by step.  Tolerance: relative L-inf <= 1e-12 per step on Sigma,
-v_r, v_phi, and relative 1e-12 on dt, disk mass and torque (FP64; the two
-sides differ only by FMA contraction and libm ulps)."""
+inputs, step by step.  Tolerance: relative L-inf <= 1e-12 per step on Sigma
+(to max|Sigma|) and on v_r, v_phi (to the max speed, so a near-zero v_r does
+not turn rounding into a large ratio), relative 1e-12 on dt and disk mass (FP64; the two sides differ
+only by FMA contraction and libm ulps).  The torque is a sum of terms that
+cancel to ~1e-3 of their magnitude, so its bound is 1e-12 times the sum of
+the absolute terms (a floating-point sum's rounding scale)."""
 import numpy as np
 import pytest
 
 import penguin_2_0_b200 as pg
-from tests._lockstep import OracleLoop, rel_linf
+from tests._lockstep import OracleLoop, rel_linf, torque_abs_scale
 
 TOL = 1e-12
 
 CASES = {
     "g128x132": dict(imax=128, jmax=132),
+    "g136x136": dict(imax=136, jmax=136),
     "g232x240": dict(imax=232, jmax=240),          # imax % 116 == 0: last radial chunk idle
     "g130x232": dict(imax=130, jmax=232),          # jmax % 116 == 0: last azimuthal chunk idle
     "g120x150_plain": dict(imax=120, jmax=150, plnt_flag=0, visc_flag=0, flat_flag=0, FARGO_flag=0,
                            kill_rin=0.0, kill_rout=0.0),
-    "g300x350": dict(imax=300, jmax=350),
+    "cfg0": dict(imax=256, jmax=768),
 }
 
 
@@ -47,15 +51,18 @@ def test_host_loop_matches_oracle(gpu, case):
         dt, mass, tq = ref.step()
         f = ref.fields()
         gdt, gmass, gtq, gf = got[s]
+        np.testing.assert_array_equal(gf["rot_j"], f["rot_j"])
+        speed = max(np.max(np.abs(f["u"])), np.max(np.abs(f["v"])))
+        e = [rel_linf(gf["r"], f["r"]), np.max(np.abs(gf["u"] - f["u"])) / speed,
+             np.max(np.abs(gf["v"] - f["v"])) / speed]
+        assert max(e) <= TOL, (case, s, e)
+        assert np.all(gf["w"] == 0.0)
         assert abs(gdt - dt) <= TOL * dt, (s, gdt, dt)
         assert abs(gmass - mass) <= TOL * abs(mass), (s, gmass, mass)
         if p.plnt_flag:
-            assert abs(gtq - tq) <= max(TOL * abs(tq), 1e-18), (s, gtq, tq)
-        np.testing.assert_array_equal(gf["rot_j"], f["rot_j"])
-        for fld in ("r", "u", "v"):
-            e = rel_linf(gf[fld], f[fld])
-            assert e <= TOL, (case, s, fld, e)
-        assert np.all(gf["w"] == 0.0)
+            scale = torque_abs_scale(f, p, pg.Planet(*[getattr(ref.planet, k) for k in
+                                                       ("m", "x", "y", "vx", "vy", "fx", "fy", "rs")]))
+            assert abs(gtq - tq) <= TOL * scale, (s, gtq, tq, scale)
 
 
 @pytest.mark.gpu

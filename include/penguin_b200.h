@@ -232,6 +232,28 @@ int64_t pg_launch_count(const pg_run *run);
 int pg_timing(pg_run *run, int on);
 int pg_timing_read(pg_run *run, double *ms_sum, int64_t *counts, int nkinds);
 
+/* ---- reduction over caller buffers, no device allocation ---------------- */
+
+/* No counterpart in the reference.  Disk mass (mode 0), radial force (8) or
+ * torque (9) of one 2D disk, in GPU_output_reduction's summation order, over
+ * device arrays the caller owns: sigma[i*row_stride + j] in physical azimuth
+ * order, per ring xc, xvol, rot_j, per column yc, yvol; *out is a device
+ * double written by the kernel on `stream` (no host copy, no sync).  For
+ * callers that must not allocate device memory (during graph capture, inside
+ * a fixed memory pool, in a time loop that allocated everything up front):
+ * the entry point calls no cudaMalloc/cudaFree; its scratch is a static
+ * __device__ array of PG_NOALLOC_MAX_RINGS doubles that every GPU loading the
+ * library keeps until exit.  imax above that limit returns PG_ERR_PARAMS.
+ * The first call on a device looks the array up with cudaGetSymbolAddress
+ * (make it before any stream capture); calls share the array, so calls that
+ * overlap on the GPU race.  Modes 8 and 9 assume a planet (plnt_flag > 0). */
+#define PG_NOALLOC_MAX_RINGS 16384
+int pg_reduce_noalloc(const double *sigma, int64_t row_stride, const double *xc,
+                      const double *xvol, const int *rot_j, const double *yc,
+                      const double *yvol, int imax, int jmax, const pg_body *planet,
+                      double exclude, int mode, double p_alpha, double sc_h,
+                      double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -137,6 +137,8 @@ def lib() -> C.CDLL:
         "pg_launch_count": (C.c_int64, [vp]),
         "pg_timing": (C.c_int, [vp, C.c_int]),
         "pg_timing_read": (C.c_int, [vp, dp, C.POINTER(C.c_int64), C.c_int]),
+        "pg_reduce_noalloc": (C.c_int, [vp, C.c_int64, vp, vp, vp, vp, vp, C.c_int, C.c_int, B,
+                                        C.c_double, C.c_int, C.c_double, C.c_double, vp, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name, None)

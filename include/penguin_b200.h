@@ -167,6 +167,13 @@ int pg_sweep2d(pg_run *run, double dt, const pg_body *planet, double frrot);
  * radial, azimuthal and polar sweeps, then rotate_rings.                  */
 int pg_sweep3d(pg_run *run, double dt, const pg_body *planet, double frrot);
 
+/* One directional sweep: axis 0 = sweepx (ppm.cu:26-160), 1 = sweepy
+ * (ppm.cu:162-307) with the FARGO integer shift applied at its store, 2 =
+ * the polar sweep of pg_sweep3d.  rot_j is not advanced: call pg_rotate
+ * (rotate_rings, ppm.cu:309-322) after the azimuthal sweep when FARGO is on. */
+int pg_sweep_axis(pg_run *run, int axis, double dt, const pg_body *planet, double frrot);
+int pg_rotate(pg_run *run);
+
 /* Wave damping toward the initial axisymmetric profile for r < kill_rin and
  * r > kill_rout.  The live reference has no damping (global.h:22); this
  * restates the dead kill_wave.cu:19-40 formula on the current layout.      */

@@ -525,11 +525,13 @@ static void evolve(oblk *B, int nmax, double dt, int axis, double FrRot, const o
       } else {
         if (G.ngeomz == 0) { B->dvol[n] = dxn; vfac[n] = 1.0; }
         else if (G.ngeomz == 5) {
+          /* cos(a) - cos(b) = 2 sin((a+b)/2) sin((b-a)/2): the value of
+           * evolve.cu:119-123 without its cancellation (the polar sweep has
+           * no reference driver to match bit for bit) */
           double delx = xa - x0;
-          double dum = cos(xa);
-          B->dvol[n] = (dum - cos(xa + dxn)) * B->rad[n];
+          B->dvol[n] = 2.0 * sin(xa + 0.5 * dxn) * sin(0.5 * dxn) * B->rad[n];
           if (delx == 0.0) vfac[n] = sin(xa);
-          else vfac[n] = (cos(x0) - dum) / delx;
+          else vfac[n] = 2.0 * sin(x0 + 0.5 * delx) * sin(0.5 * delx) / delx;
         }
       }
     }
@@ -574,7 +576,10 @@ static void remap(oblk *B, int nmax, int axis, double *al, double *da, double *a
       else lvol = (xa - x0) * B->rad[n];
     } else {
       if (G.ngeomz == 0) lvol = xa - x0;
-      else if (G.ngeomz == 5) lvol = (cos(x0) - cos(xa)) * B->rad[n];
+      else if (G.ngeomz == 5) {
+        double d = xa - x0;   /* remap.cu:221 without cancellation */
+        lvol = 2.0 * sin(x0 + 0.5 * d) * sin(0.5 * d) * B->rad[n];
+      }
     }
     B->lvol[n] = lvol;
     B->dxf[n] = xa - x0;
@@ -920,11 +925,10 @@ static void sweepz_block(orc_run *R, oblk *B, int i_rad, int j0, double dt, cons
       double rad = c->xc;
       double zc = c->zc, za = c->z, dz = c->dz, zvol = c->zvol;
       if (mir[i]) {
-        /* mirror image across zmax: face at 2 zmax - (z + dz) */
-        double zmax = G.zmax;
-        za = 2.0 * zmax - (c->z + c->dz);
-        zc = za + 0.5 * dz;
-        zvol = cos(za) - cos(za + dz);
+        /* mirror layer: the state of layer 2 kmax - 1 - k, the geometry of
+         * the fixed upper ring at this k (init.cpp:485-488) */
+        const oring *tg = &R->top[(k_ring - kmax) + NPAD * i_rad];
+        za = tg->z; dz = tg->dz; zc = tg->zc; zvol = tg->zvol;
       }
       (void)k_ring;
       B->rad[i] = rad;

@@ -121,6 +121,8 @@ def lib() -> C.CDLL:
         "pg_sweep2d": (C.c_int, [vp, C.c_double, B, C.c_double]),
         "pg_sweep3d": (C.c_int, [vp, C.c_double, B, C.c_double]),
         "pg_damp": (C.c_int, [vp, C.c_double]),
+        "pg_sweep_axis": (C.c_int, [vp, C.c_int, C.c_double, B, C.c_double]),
+        "pg_rotate": (C.c_int, [vp]),
         "pg_reduce": (C.c_int, [vp, B, C.c_double, C.c_int, dp]),
         "pg_init_planet": (C.c_int, [P, B, dp]),
         "pg_set_M_p": (C.c_double, [P, C.c_double]),

@@ -19,8 +19,8 @@ struct CellIn {
   double dvol0;  // Eulerian cell volume along the sweep
 };
 
-template <int AXIS, bool SPH>
-__device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, const ChunkShm &S,
+template <int AXIS, bool SPH, class SHM>
+__device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, const SHM &S,
                                            const Body &pl, const Phys &ph, double &ftot) {
   if (AXIS == 0) {
     // get_fx_bound forces.cu:185-224 at the left face xa0[n]
@@ -58,9 +58,9 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
 }
 
 // get_fx / get_fy / get_fz at a cell centre (forces.cu:226-372)
-template <int AXIS, bool SPH>
+template <int AXIS, bool SPH, class SHM>
 __device__ __forceinline__ double centre_force(int n, double dt, double rad, double azi, double pol,
-                                               const ChunkShm &S, const Body &pl, const Phys &ph) {
+                                               const SHM &S, const Body &pl, const Phys &ph) {
   if (AXIS == 0) {
     double grav;
     if (!SPH) {
@@ -91,8 +91,8 @@ __device__ __forceinline__ double centre_force(int n, double dt, double rad, dou
 // The ppmlr chain for one chunk.  All threads of the CTA call it (it has
 // barriers); cells n >= nmax take no part in any phase.  On return r, u, v
 // (and w when THREED) hold the Lagrange-remapped values for 6 <= n < nmax-6.
-template <int AXIS, bool SPH, bool THREED>
-__device__ __forceinline__ void ppm_chunk(ChunkShm &S, int n, int nmax, double dt, double FrRot,
+template <int AXIS, bool SPH, bool THREED, class SHM>
+__device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, double FrRot,
                                           const CellIn &c, const Body &pl, const Phys &ph) {
   const bool act = n < nmax;
   double flat = 0.0;
@@ -178,7 +178,7 @@ __device__ __forceinline__ void ppm_chunk(ChunkShm &S, int n, int nmax, double d
 
   // ---- evolve evolve.cu:3-166 (vfac = tmp1) ----
   double *vfac = S.tmp1;
-  const double xa0n = S.xa0[n < AP ? n : 0];
+  const double xa0n = S.xa0[n];
   double xa = xa0n, dvol = c.dvol0, dtdm = 0.0, fto1 = 0.0, fto2 = 0.0;
   if (act) vfac[n] = S.xa0[n] + 0.5 * S.dx0[n];
   __syncthreads();
@@ -221,11 +221,13 @@ __device__ __forceinline__ void ppm_chunk(ChunkShm &S, int n, int nmax, double d
     } else if (AXIS == 1) {
       dvol = dxn * c.rad; vfac[n] = 1.0;
     } else {
+      // evolve.cu:117-124 with cos(a) - cos(b) written as
+      // 2 sin((a+b)/2) sin((b-a)/2): the same value without the
+      // cancellation that makes the reference's form depend on libm ulps
       double delx = xa - xa0n;
-      double dum = cos(xa);
-      dvol = (dum - cos(xa + dxn)) * c.rad;
+      dvol = 2.0 * sin(xa + 0.5 * dxn) * sin(0.5 * dxn) * c.rad;
       if (delx == 0.0) vfac[n] = sin(xa);
-      else vfac[n] = (cos(xa0n) - dum) / delx;
+      else vfac[n] = 2.0 * sin(xa0n + 0.5 * delx) * sin(0.5 * delx) / delx;
     }
   }
   __syncthreads();
@@ -248,7 +250,9 @@ __device__ __forceinline__ void ppm_chunk(ChunkShm &S, int n, int nmax, double d
   } else if (AXIS == 1) {
     lvol = (xa - xa0n) * c.rad;
   } else {
-    lvol = (cos(xa0n) - cos(xa)) * c.rad;
+    // remap.cu:221, cancellation-free form of (cos(xa0) - cos(xa)) * rad
+    double d = xa - xa0n;
+    lvol = 2.0 * sin(xa0n + 0.5 * d) * sin(0.5 * d) * c.rad;
   }
   double dxf = xa - xa0n;
   const bool delC = (dxf >= 0.0);

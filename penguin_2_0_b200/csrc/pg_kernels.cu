@@ -72,13 +72,13 @@ __device__ __forceinline__ bool load_step(const SweepCtl &c, StepIn &s) {
 
 // ---------------------------------------------------------------------------
 // radial sweep
-template <bool SPH, bool THREED>
-__global__ void __launch_bounds__(ARR) k_sweep_x(Tables T, Planes P, Phys ph, SweepCtl ctl) {
-  __shared__ ChunkShm S;
+template <bool SPH, bool THREED, int NT>
+__global__ void __launch_bounds__(NT) k_sweep_x(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
+  __shared__ ChunkShmT<NT> S;
   StepIn st;
   if (!load_step(ctl, st)) return;
   const int n = threadIdx.x;
-  const int j0 = blockIdx.x, l = blockIdx.y, k = blockIdx.z;
+  const int j0 = blockIdx.x, l = blockIdx.y + l0, k = blockIdx.z;
   const bool last = (l == T.cx.loop - 1);
   const int nphi = T.nphi, nrg = T.nrg;
   if (last && T.cx.stuck) {
@@ -163,19 +163,19 @@ __global__ void __launch_bounds__(ARR) k_sweep_x(Tables T, Planes P, Phys ph, Sw
 
 // ---------------------------------------------------------------------------
 // azimuthal sweep with the FARGO shift at the store and the fused epilogue
-template <bool SPH, bool THREED>
-__global__ void __launch_bounds__(ARR) k_sweep_y(Tables T, Planes P, Phys ph, SweepCtl ctl) {
-  __shared__ ChunkShm S;
-  __shared__ double red[ARR / 32];
+template <bool SPH, bool THREED, int NT>
+__global__ void __launch_bounds__(NT) k_sweep_y(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
+  __shared__ ChunkShmT<NT> S;
+  __shared__ double red[NT / 32];
   StepIn st;
   if (!load_step(ctl, st)) return;
   const int n = threadIdx.x;
-  const int l = blockIdx.x, i = blockIdx.y, k = blockIdx.z;
+  const int l = blockIdx.x + l0, i = blockIdx.y, k = blockIdx.z;
   const int nphi = T.nphi, nrg = T.nrg;
   const int row = i + NPAD;
   const int rk = k * nrg + row;
   const size_t base = (size_t)rk * nphi;
-  const int inc = T.inc_j[rk];
+  const int inc = ctl.shift ? T.inc_j[rk] : 0;
   const bool last = (l == T.cy.loop - 1);
   const double rad = T.rxc[row];
   const double rad_cyl = T.radc[rk];
@@ -316,12 +316,13 @@ __global__ void __launch_bounds__(ARR) k_sweep_y(Tables T, Planes P, Phys ph, Sw
 // v <- v_r, w <- r sin(theta) v_phi (so get_fz's w^2 cos/(r sin)^3 is the
 // centrifugal term); viscosity follows device_viscosity_p's pattern on the
 // arc length r*theta.
-__global__ void __launch_bounds__(ARR) k_sweep_z(Tables T, Planes P, Phys ph, SweepCtl ctl, int ntop) {
-  __shared__ ChunkShm S;
+template <int NT>
+__global__ void __launch_bounds__(NT) k_sweep_z(Tables T, Planes P, Phys ph, SweepCtl ctl, int ntop, int l0) {
+  __shared__ ChunkShmT<NT> S;
   StepIn st;
   if (!load_step(ctl, st)) return;
   const int n = threadIdx.x;
-  const int i = blockIdx.x, j0 = blockIdx.y, l = blockIdx.z;
+  const int i = blockIdx.x, j0 = blockIdx.y, l = blockIdx.z + l0;
   const int nphi = T.nphi, nrg = T.nrg, nk = T.nk;
   const int row = i + NPAD;
   const bool last = (l == T.cz.loop - 1);
@@ -329,7 +330,9 @@ __global__ void __launch_bounds__(ARR) k_sweep_z(Tables T, Planes P, Phys ph, Sw
     int k = REAL * l + n;
     if (n < REAL && k < nk) {
       size_t idx = ((size_t)k * nrg + row) * nphi + j0;
-      P.ro[idx] = P.r[idx]; P.uo[idx] = P.u[idx]; P.vo[idx] = P.v[idx]; P.wo[idx] = P.w[idx];
+      int inc = ctl.shift ? T.inc_j[k * nrg + row] : 0;
+      size_t o = ((size_t)k * nrg + row) * nphi + wrapm(j0 + inc, nphi);
+      P.ro[o] = P.r[idx]; P.uo[o] = P.u[idx]; P.vo[o] = P.v[idx]; P.wo[o] = P.w[idx];
     }
     return;
   }
@@ -394,8 +397,10 @@ __global__ void __launch_bounds__(ARR) k_sweep_z(Tables T, Planes P, Phys ph, Sw
     if (act) {
       S.xa0[n] *= rad;
       rho = S.r[n];
-      int kk = kr < 0 ? 0 : (kr >= nk ? nk - 1 : kr);
-      nr = T.nu[kk * nrg + row] * rho;
+      // nu at this layer's r sin(theta): the table for interior layers, the
+      // same expression (get_nu disk_profile.cu:149-152) for ghost layers
+      double nu = (kr >= 0 && kr < nk) ? T.nu[kr * nrg + row] : ph.vis_nu * pow(rad_cyl, ph.p_alpha);
+      nr = nu * rho;
       S.dx0[n] = nr;
     }
     __syncthreads();
@@ -411,10 +416,14 @@ __global__ void __launch_bounds__(ARR) k_sweep_z(Tables T, Planes P, Phys ph, Sw
     if (n >= NPAD && n < lim - NPAD) { S.u[n] = ddu; S.v[n] = ddv; }
   }
   if (n >= NPAD && n < lim - NPAD) {
-    P.ro[idx] = S.r[n];
-    P.wo[idx] = S.u[n];
-    P.uo[idx] = S.v[n];
-    P.vo[idx] = S.w[n] / rad_cyl;
+    // the polar sweep is the last of a 3D step: the FARGO integer shift of
+    // each layer (rotate_rings, ppm.cu:309-322) is applied at this store
+    int inc = ctl.shift ? T.inc_j[kr * nrg + row] : 0;
+    size_t o = (size_t)(kr * nrg + row) * nphi + wrapm(j0 + inc, nphi);
+    P.ro[o] = S.r[n];
+    P.wo[o] = S.u[n];
+    P.uo[o] = S.v[n];
+    P.vo[o] = S.w[n] / rad_cyl;
   }
 }
 
@@ -837,22 +846,76 @@ __global__ void k_poststep(DevClock *clk, Tables T) {
 namespace pgk {
 using namespace pgd;
 
+// CTA size for a chunk of `lim` active cells
+static inline int cta_for(int lim) { return lim <= 32 ? 32 : (lim <= 64 ? 64 : 128); }
+
 void sweep_x(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
-  dim3 grid(T.nphi, T.cx.loop, T.nk);
-  if (ndim == 3) k_sweep_x<true, true><<<grid, ARR, 0, s>>>(T, P, ph, c);
-  else k_sweep_x<false, false><<<grid, ARR, 0, s>>>(T, P, ph, c);
+  const Chunking &ch = T.cx;
+  int full = ch.stuck ? ch.loop : ch.loop - 1;
+  if (full > 0) {
+    dim3 grid(T.nphi, full, T.nk);
+    if (ndim == 3) k_sweep_x<true, true, 128><<<grid, 128, 0, s>>>(T, P, ph, c, 0);
+    else k_sweep_x<false, false, 128><<<grid, 128, 0, s>>>(T, P, ph, c, 0);
+  }
+  if (!ch.stuck) {
+    dim3 grid(T.nphi, 1, T.nk);
+    int nt = cta_for(ch.lim_last);
+    int l0 = ch.loop - 1;
+    if (ndim == 3) {
+      if (nt == 32) k_sweep_x<true, true, 32><<<grid, 32, 0, s>>>(T, P, ph, c, l0);
+      else if (nt == 64) k_sweep_x<true, true, 64><<<grid, 64, 0, s>>>(T, P, ph, c, l0);
+      else k_sweep_x<true, true, 128><<<grid, 128, 0, s>>>(T, P, ph, c, l0);
+    } else {
+      if (nt == 32) k_sweep_x<false, false, 32><<<grid, 32, 0, s>>>(T, P, ph, c, l0);
+      else if (nt == 64) k_sweep_x<false, false, 64><<<grid, 64, 0, s>>>(T, P, ph, c, l0);
+      else k_sweep_x<false, false, 128><<<grid, 128, 0, s>>>(T, P, ph, c, l0);
+    }
+  }
 }
 
 void sweep_y(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
-  dim3 grid(T.cy.loop, T.nr, T.nk);
-  if (ndim == 3) k_sweep_y<true, true><<<grid, ARR, 0, s>>>(T, P, ph, c);
-  else k_sweep_y<false, false><<<grid, ARR, 0, s>>>(T, P, ph, c);
+  const Chunking &ch = T.cy;
+  int full = ch.stuck ? ch.loop : ch.loop - 1;
+  if (full > 0) {
+    dim3 grid(full, T.nr, T.nk);
+    if (ndim == 3) k_sweep_y<true, true, 128><<<grid, 128, 0, s>>>(T, P, ph, c, 0);
+    else k_sweep_y<false, false, 128><<<grid, 128, 0, s>>>(T, P, ph, c, 0);
+  }
+  if (!ch.stuck) {
+    dim3 grid(1, T.nr, T.nk);
+    int nt = cta_for(ch.lim_last);
+    int l0 = ch.loop - 1;
+    if (ndim == 3) {
+      if (nt == 32) k_sweep_y<true, true, 32><<<grid, 32, 0, s>>>(T, P, ph, c, l0);
+      else if (nt == 64) k_sweep_y<true, true, 64><<<grid, 64, 0, s>>>(T, P, ph, c, l0);
+      else k_sweep_y<true, true, 128><<<grid, 128, 0, s>>>(T, P, ph, c, l0);
+    } else {
+      if (nt == 32) k_sweep_y<false, false, 32><<<grid, 32, 0, s>>>(T, P, ph, c, l0);
+      else if (nt == 64) k_sweep_y<false, false, 64><<<grid, 64, 0, s>>>(T, P, ph, c, l0);
+      else k_sweep_y<false, false, 128><<<grid, 128, 0, s>>>(T, P, ph, c, l0);
+    }
+  }
 }
 
 void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s) {
-  dim3 grid(T.nr, T.nphi, T.cz.loop);
-  k_sweep_z<<<grid, ARR, 0, s>>>(T, P, ph, c, ntop);
+  const Chunking &ch = T.cz;
+  int full = ch.stuck ? ch.loop : ch.loop - 1;
+  if (full > 0) {
+    dim3 grid(T.nr, T.nphi, full);
+    k_sweep_z<128><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, 0);
+  }
+  if (!ch.stuck) {
+    dim3 grid(T.nr, T.nphi, 1);
+    int nt = cta_for(ch.lim_last);
+    int l0 = ch.loop - 1;
+    if (nt == 32) k_sweep_z<32><<<grid, 32, 0, s>>>(T, P, ph, c, ntop, l0);
+    else if (nt == 64) k_sweep_z<64><<<grid, 64, 0, s>>>(T, P, ph, c, ntop, l0);
+    else k_sweep_z<128><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, l0);
+  }
 }
+
+// kernels launched by one sweep_* call
+int sweep_launches(const Chunking &ch) { return (ch.stuck || ch.loop == 1) ? 1 : 2; }
 
 void cfl_full(const Tables &T, const double *r, const double *u, const double *v, const double *w,
               const double *p0, const Phys &ph, double frrot, int ndim, unsigned long long *out,

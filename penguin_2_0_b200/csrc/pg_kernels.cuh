@@ -69,6 +69,7 @@ struct SweepCtl {
   Body planet;
   DevClock *clk;      // non-null: read dt/planet/frrot from the clock, honour halt
   int fuse;           // sweepy epilogue: damping + CFL + finiteness check
+  int shift;          // store at (j + inc_j) mod jmax: the last sweep of a step
 };
 
 }  // namespace pgd
@@ -81,6 +82,7 @@ void tables(const Tables &T, const Phys &ph, int ndim, double kill_rin, double k
 void sweep_x(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s);
 void sweep_y(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s);
 void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s);
+int sweep_launches(const Chunking &ch);
 void cfl_full(const Tables &T, const double *r, const double *u, const double *v, const double *w,
               const double *p0, const Phys &ph, double frrot, int ndim, unsigned long long *out,
               cudaStream_t s);

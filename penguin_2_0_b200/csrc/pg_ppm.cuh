@@ -52,10 +52,12 @@ struct Par { double c0, c1, c2, c3, c4; };
 
 // Shared arrays of one chunk: the sweep kernel's (ppm.cu:38-39) and
 // ppmlr's (ppmlr.cu:7-10).  q only serves as parabola storage (al) because
-// the q = p/rho remap is dead in EOS 0.
-struct ChunkShm {
-  double r[AP], p[AP], u[AP], v[AP], w[AP], xa0[AP], dx0[AP];
-  double q[AP], dx[AP], umid[AP], pmid[AP], tmp1[AP];
+// the q = p/rho remap is dead in EOS 0.  NT is the CTA size: 128 for full
+// chunks, 64 or 32 for a short last chunk (lim <= NT).
+template <int NT>
+struct ChunkShmT {
+  double r[NT + 2], p[NT + 2], u[NT + 2], v[NT + 2], w[NT + 2], xa0[NT + 2], dx0[NT + 2];
+  double q[NT + 2], dx[NT + 2], umid[NT + 2], pmid[NT + 2], tmp1[NT + 2];
 };
 
 // ---- star + planet gravity, forces.cu:23-182 (non-barycentric frame) ------

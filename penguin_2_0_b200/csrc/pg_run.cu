@@ -502,8 +502,13 @@ static pgd::SweepCtl host_ctl(double dt, const pg_body *pl, double frrot) {
   c.planet = pgd::Body{pl->m, pl->x, pl->y, pl->vx, pl->vy, pl->fx, pl->fy, pl->rs};
   c.clk = nullptr;
   c.fuse = 0;
+  c.shift = 0;
   return c;
 }
+
+static int nx(pg_run *run) { return pgk::sweep_launches(run->T.cx); }
+static int ny(pg_run *run) { return pgk::sweep_launches(run->T.cy); }
+static int nz(pg_run *run) { return pgk::sweep_launches(run->T.cz); }
 
 int pg_sweep2d(pg_run *run, double dt, const pg_body *planet, double frrot) {
   if (!run || !planet) return PG_ERR_ARG;
@@ -513,10 +518,11 @@ int pg_sweep2d(pg_run *run, double dt, const pg_body *planet, double frrot) {
   pgd::SweepCtl c = host_ctl(dt, planet, frrot);
   cudaStream_t s = run->stream;
   pgk::sweep_x(run->T, planes_fwd(run, run->cur, run->p0_live ? run->p0 : nullptr), run->ph, c, 2, s);
+  c.shift = 1;
   pgk::sweep_y(run->T, planes_fwd(run, 1 - run->cur, nullptr), run->ph, c, 2, s);
   if (run->P.FARGO_flag > 0) pgk::rotate(run->T, nullptr, s);
   run->p0_live = false;
-  return check_launch(run, run->P.FARGO_flag > 0 ? 3 : 2);
+  return check_launch(run, nx(run) + ny(run) + (run->P.FARGO_flag > 0 ? 1 : 0));
 }
 
 int pg_sweep3d(pg_run *run, double dt, const pg_body *planet, double frrot) {
@@ -529,11 +535,48 @@ int pg_sweep3d(pg_run *run, double dt, const pg_body *planet, double frrot) {
   int a = run->cur;
   pgk::sweep_x(run->T, planes_fwd(run, a, run->p0_live ? run->p0 : nullptr), run->ph, c, 3, s);
   pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 3, s);
+  c.shift = 1;   // the polar sweep is the last one: it applies the FARGO shift
   pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, run->P.ntop, s);
   if (run->P.FARGO_flag > 0) pgk::rotate(run->T, nullptr, s);
   run->cur = 1 - a;
   run->p0_live = false;
-  return check_launch(run, run->P.FARGO_flag > 0 ? 4 : 3);
+  return check_launch(run, nx(run) + ny(run) + nz(run) + (run->P.FARGO_flag > 0 ? 1 : 0));
+}
+
+int pg_sweep_axis(pg_run *run, int axis, double dt, const pg_body *planet, double frrot) {
+  if (!run || !planet) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  if (axis < 0 || axis > 2 || (axis == 2 && run->P.ndim != 3)) return fail(run, PG_ERR_ARG, "bad sweep axis");
+  CK(cudaSetDevice(run->dev));
+  pgd::SweepCtl c = host_ctl(dt, planet, frrot);
+  cudaStream_t s = run->stream;
+  int a = run->cur;
+  // the FARGO shift goes with the last sweep of a step: azimuthal in 2D,
+  // polar in 3D.  The dump's p is used only by a leading radial sweep.
+  int n = 0;
+  if (axis == 0) {
+    pgk::sweep_x(run->T, planes_fwd(run, a, run->p0_live ? run->p0 : nullptr), run->ph, c, run->P.ndim, s);
+    n = nx(run);
+  } else if (axis == 1) {
+    c.shift = run->P.ndim == 2;
+    pgk::sweep_y(run->T, planes_fwd(run, a, nullptr), run->ph, c, run->P.ndim, s);
+    n = ny(run);
+  } else {
+    c.shift = 1;
+    pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, run->P.ntop, s);
+    n = nz(run);
+  }
+  run->cur = 1 - a;
+  run->p0_live = false;
+  return check_launch(run, n);
+}
+
+int pg_rotate(pg_run *run) {
+  if (!run) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  CK(cudaSetDevice(run->dev));
+  pgk::rotate(run->T, nullptr, run->stream);
+  return check_launch(run, 1);
 }
 
 int pg_damp(pg_run *run, double dt) {
@@ -696,6 +739,7 @@ static int enqueue_step(pg_run *run, bool first_p0) {
   pgd::SweepCtl c{};
   c.clk = run->clk;
   c.fuse = 0;
+  c.shift = 0;
   int a = run->cur;
   int n = 0;
   const bool tm = run->timing;
@@ -703,20 +747,22 @@ static int enqueue_step(pg_run *run, bool first_p0) {
   if (tm && ev_pair(run, 3, e_step)) return fail(run, PG_ERR_CUDA, "event record");
   pgk::prestep(run->clk, run->T, P.FARGO_flag, s); n++;
   if (tm && ev_pair(run, 0, e_k)) return fail(run, PG_ERR_CUDA, "event record");
-  pgk::sweep_x(run->T, planes_fwd(run, a, first_p0 ? run->p0 : nullptr), run->ph, c, P.ndim, s); n++;
+  pgk::sweep_x(run->T, planes_fwd(run, a, first_p0 ? run->p0 : nullptr), run->ph, c, P.ndim, s); n += nx(run);
   if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
   if (P.ndim == 2) {
     c.fuse = 1;
+    c.shift = 1;
     if (tm && ev_pair(run, 1, e_k)) return fail(run, PG_ERR_CUDA, "event record");
-    pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 2, s); n++;
+    pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 2, s); n += ny(run);
     if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
   } else {
     if (tm && ev_pair(run, 1, e_k)) return fail(run, PG_ERR_CUDA, "event record");
-    pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 3, s); n++;
+    pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 3, s); n += ny(run);
     if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
-    // 3D: damping and CFL after the polar sweep
+    // 3D: the polar sweep applies the FARGO shift; damping and CFL follow it
     if (tm && ev_pair(run, 2, e_k)) return fail(run, PG_ERR_CUDA, "event record");
-    pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, P.ntop, s); n++;
+    c.shift = 1;
+    pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, P.ntop, s); n += nz(run);
     if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     double **cp = run->planes[1 - a];
     pgk::damp_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->clk, s); n++;

@@ -311,6 +311,18 @@ def bundle_sweep3D(run: Run, dt: float, planet: Planet, FrRot: float = 0.0):
     _check(_lib.lib().pg_sweep3d(run._h, dt, C.byref(b), FrRot), run, "pg_sweep3d")
 
 
+def sweep_axis(run: Run, axis: int, dt: float, planet: Planet, FrRot: float = 0.0):
+    """One directional sweep: 0 = sweepx (ppm.cu:26), 1 = sweepy (ppm.cu:162,
+    FARGO shift at the store), 2 = the polar sweep (3D)."""
+    b = planet.to_c()
+    _check(_lib.lib().pg_sweep_axis(run._h, axis, dt, C.byref(b), FrRot), run, "pg_sweep_axis")
+
+
+def rotate_rings(run: Run):
+    """rotate_rings (ppm.cu:309-322): rot_j += inc_j."""
+    _check(_lib.lib().pg_rotate(run._h), run, "pg_rotate")
+
+
 def GPU_output_reduction(run: Run, planet: Planet, exclude: float = 0.0, mode: int = 0) -> float:
     b = planet.to_c()
     out = C.c_double(0.0)

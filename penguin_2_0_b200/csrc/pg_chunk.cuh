@@ -124,7 +124,10 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   }
 
   // ---- states states.cu:3-73 ----
-  // al = q, da = dx, a6 = tmp1, cs = umid, csfac = pmid (ppmlr.cu:30-33)
+  // al = q, da = dx, a6 = tmp1, cs = umid, csfac = pmid (ppmlr.cu:30-33).
+  // paraset runs per cell as in the reference: tabulating its Eulerian
+  // coefficients in a separate kernel changes their FMA contraction (the
+  // last bits), which then shows up at 1e-12 in v_r.
   const double hdt = 0.5 * dt;
   Par par;
   paraset(n, 0, nmax, par, S.dx0, S.q, S.dx, S.tmp1);

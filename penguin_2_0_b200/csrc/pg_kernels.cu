@@ -72,8 +72,8 @@ __device__ __forceinline__ bool load_step(const SweepCtl &c, StepIn &s) {
 
 // ---------------------------------------------------------------------------
 // radial sweep
-template <bool SPH, bool THREED, int NT>
-__global__ void __launch_bounds__(NT) k_sweep_x(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
+template <bool SPH, bool THREED, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sweep_x(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
   __shared__ ChunkShmT<NT> S;
   StepIn st;
   if (!load_step(ctl, st)) return;
@@ -163,8 +163,8 @@ __global__ void __launch_bounds__(NT) k_sweep_x(Tables T, Planes P, Phys ph, Swe
 
 // ---------------------------------------------------------------------------
 // azimuthal sweep with the FARGO shift at the store and the fused epilogue
-template <bool SPH, bool THREED, int NT>
-__global__ void __launch_bounds__(NT) k_sweep_y(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
+template <bool SPH, bool THREED, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sweep_y(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
   __shared__ ChunkShmT<NT> S;
   __shared__ double red[NT / 32];
   StepIn st;
@@ -316,8 +316,8 @@ __global__ void __launch_bounds__(NT) k_sweep_y(Tables T, Planes P, Phys ph, Swe
 // v <- v_r, w <- r sin(theta) v_phi (so get_fz's w^2 cos/(r sin)^3 is the
 // centrifugal term); viscosity follows device_viscosity_p's pattern on the
 // arc length r*theta.
-template <int NT>
-__global__ void __launch_bounds__(NT) k_sweep_z(Tables T, Planes P, Phys ph, SweepCtl ctl, int ntop, int l0) {
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sweep_z(Tables T, Planes P, Phys ph, SweepCtl ctl, int ntop, int l0) {
   __shared__ ChunkShmT<NT> S;
   StepIn st;
   if (!load_step(ctl, st)) return;
@@ -849,51 +849,57 @@ using namespace pgd;
 // CTA size for a chunk of `lim` active cells
 static inline int cta_for(int lim) { return lim <= 32 ? 32 : (lim <= 64 ? 64 : 128); }
 
+// Occupancy variant of the 128-thread sweeps: MINB 1 lets the compiler keep
+// ~76 registers (6 CTAs per SM), MINB 8 caps them at 64 (8 CTAs per SM, a
+// few spilled values).  Chosen per run (pg_run's tuning, PG_SWEEP_OCC).
+#define PG_LAUNCH_X(SPHV, TD, NTV, grid, l0)                                                   \
+  do {                                                                                          \
+    if ((NTV) == 128 && occ8) k_sweep_x<SPHV, TD, 128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, l0); \
+    else if ((NTV) == 128) k_sweep_x<SPHV, TD, 128, 1><<<grid, 128, 0, s>>>(T, P, ph, c, l0);  \
+    else if ((NTV) == 64) k_sweep_x<SPHV, TD, 64, 1><<<grid, 64, 0, s>>>(T, P, ph, c, l0);     \
+    else k_sweep_x<SPHV, TD, 32, 1><<<grid, 32, 0, s>>>(T, P, ph, c, l0);                      \
+  } while (0)
+#define PG_LAUNCH_Y(SPHV, TD, NTV, grid, l0)                                                   \
+  do {                                                                                          \
+    if ((NTV) == 128 && occ8) k_sweep_y<SPHV, TD, 128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, l0); \
+    else if ((NTV) == 128) k_sweep_y<SPHV, TD, 128, 1><<<grid, 128, 0, s>>>(T, P, ph, c, l0);  \
+    else if ((NTV) == 64) k_sweep_y<SPHV, TD, 64, 1><<<grid, 64, 0, s>>>(T, P, ph, c, l0);     \
+    else k_sweep_y<SPHV, TD, 32, 1><<<grid, 32, 0, s>>>(T, P, ph, c, l0);                      \
+  } while (0)
+
 void sweep_x(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
   const Chunking &ch = T.cx;
+  const int occ8 = T.occ8;
   int full = ch.stuck ? ch.loop : ch.loop - 1;
   if (full > 0) {
     dim3 grid(T.nphi, full, T.nk);
-    if (ndim == 3) k_sweep_x<true, true, 128><<<grid, 128, 0, s>>>(T, P, ph, c, 0);
-    else k_sweep_x<false, false, 128><<<grid, 128, 0, s>>>(T, P, ph, c, 0);
+    if (ndim == 3) PG_LAUNCH_X(true, true, 128, grid, 0);
+    else PG_LAUNCH_X(false, false, 128, grid, 0);
   }
   if (!ch.stuck) {
     dim3 grid(T.nphi, 1, T.nk);
     int nt = cta_for(ch.lim_last);
     int l0 = ch.loop - 1;
-    if (ndim == 3) {
-      if (nt == 32) k_sweep_x<true, true, 32><<<grid, 32, 0, s>>>(T, P, ph, c, l0);
-      else if (nt == 64) k_sweep_x<true, true, 64><<<grid, 64, 0, s>>>(T, P, ph, c, l0);
-      else k_sweep_x<true, true, 128><<<grid, 128, 0, s>>>(T, P, ph, c, l0);
-    } else {
-      if (nt == 32) k_sweep_x<false, false, 32><<<grid, 32, 0, s>>>(T, P, ph, c, l0);
-      else if (nt == 64) k_sweep_x<false, false, 64><<<grid, 64, 0, s>>>(T, P, ph, c, l0);
-      else k_sweep_x<false, false, 128><<<grid, 128, 0, s>>>(T, P, ph, c, l0);
-    }
+    if (ndim == 3) PG_LAUNCH_X(true, true, nt, grid, l0);
+    else PG_LAUNCH_X(false, false, nt, grid, l0);
   }
 }
 
 void sweep_y(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
   const Chunking &ch = T.cy;
+  const int occ8 = T.occ8;
   int full = ch.stuck ? ch.loop : ch.loop - 1;
   if (full > 0) {
     dim3 grid(full, T.nr, T.nk);
-    if (ndim == 3) k_sweep_y<true, true, 128><<<grid, 128, 0, s>>>(T, P, ph, c, 0);
-    else k_sweep_y<false, false, 128><<<grid, 128, 0, s>>>(T, P, ph, c, 0);
+    if (ndim == 3) PG_LAUNCH_Y(true, true, 128, grid, 0);
+    else PG_LAUNCH_Y(false, false, 128, grid, 0);
   }
   if (!ch.stuck) {
     dim3 grid(1, T.nr, T.nk);
     int nt = cta_for(ch.lim_last);
     int l0 = ch.loop - 1;
-    if (ndim == 3) {
-      if (nt == 32) k_sweep_y<true, true, 32><<<grid, 32, 0, s>>>(T, P, ph, c, l0);
-      else if (nt == 64) k_sweep_y<true, true, 64><<<grid, 64, 0, s>>>(T, P, ph, c, l0);
-      else k_sweep_y<true, true, 128><<<grid, 128, 0, s>>>(T, P, ph, c, l0);
-    } else {
-      if (nt == 32) k_sweep_y<false, false, 32><<<grid, 32, 0, s>>>(T, P, ph, c, l0);
-      else if (nt == 64) k_sweep_y<false, false, 64><<<grid, 64, 0, s>>>(T, P, ph, c, l0);
-      else k_sweep_y<false, false, 128><<<grid, 128, 0, s>>>(T, P, ph, c, l0);
-    }
+    if (ndim == 3) PG_LAUNCH_Y(true, true, nt, grid, l0);
+    else PG_LAUNCH_Y(false, false, nt, grid, l0);
   }
 }
 
@@ -902,15 +908,17 @@ void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c
   int full = ch.stuck ? ch.loop : ch.loop - 1;
   if (full > 0) {
     dim3 grid(T.nr, T.nphi, full);
-    k_sweep_z<128><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, 0);
+    if (T.occ8) k_sweep_z<128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, 0);
+    else k_sweep_z<128, 1><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, 0);
   }
   if (!ch.stuck) {
     dim3 grid(T.nr, T.nphi, 1);
     int nt = cta_for(ch.lim_last);
     int l0 = ch.loop - 1;
-    if (nt == 32) k_sweep_z<32><<<grid, 32, 0, s>>>(T, P, ph, c, ntop, l0);
-    else if (nt == 64) k_sweep_z<64><<<grid, 64, 0, s>>>(T, P, ph, c, ntop, l0);
-    else k_sweep_z<128><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, l0);
+    if (nt == 32) k_sweep_z<32, 1><<<grid, 32, 0, s>>>(T, P, ph, c, ntop, l0);
+    else if (nt == 64) k_sweep_z<64, 1><<<grid, 64, 0, s>>>(T, P, ph, c, ntop, l0);
+    else if (T.occ8) k_sweep_z<128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, l0);
+    else k_sweep_z<128, 1><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, l0);
   }
 }
 

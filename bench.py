@@ -49,9 +49,12 @@ WORKLOADS = {
     # name: (config index, overrides, description)
     "cfg0": (0, {}, "2D r-phi disk 256x768 FP64, planet q=1e-3, FARGO, damping (configs[0])"),
     "cfg1": (1, {}, "3D spherical disk 128x1024x32 FP64, reflecting midplane (configs[1])"),
-    "cfg2": (2, {}, "2D r-phi disk 1024x3072 FP64, same disk (configs[2] grid)"),
+    "cfg2": (2, {}, "2D r-phi disk 1024x3072 FP32 planes (precision form), same disk and planet"),
+    "cfg2_fp64": (2, {"precision": 0}, "2D r-phi disk 1024x3072 FP64, same disk and planet"),
+    "cfg0_fp32": (0, {"precision": 1}, "2D r-phi disk 256x768 FP32 planes, planet q=1e-3"),
     "big": (0, {"imax": 4096, "jmax": 12288}, "2D r-phi disk 4096x12288 FP64, same disk"),
     "prof": (0, {"imax": 2048, "jmax": 6144}, "2D r-phi disk 2048x6144 FP64 (profiling case, > L2)"),
+    "prof32": (0, {"imax": 2048, "jmax": 6144, "precision": 1}, "2D r-phi disk 2048x6144 FP32 planes (> L2)"),
 }
 
 
@@ -238,7 +241,7 @@ def main():
         print(json.dumps({"profile": args.workload, "steps": int(c.ncycle), "status": int(c.status)}))
         run.close()
         return
-    l2_resident = args.workload == "cfg0"
+    l2_resident = args.workload in ("cfg0", "cfg0_fp32")
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") if l2_resident else None
 
     # warm-up (builds the step graph too)
@@ -295,7 +298,8 @@ def main():
     mean = {kinds[i]: kms[i] / kcnt[i] for i in range(3) if kcnt[i]}
     top = max(mean, key=mean.get)
     nfield = 4 if p.ndim == 3 else 3
-    bytes_per_launch = 2 * nfield * 8 * cells
+    esize = 4 if p.precision == 1 else 8
+    bytes_per_launch = 2 * nfield * esize * cells
     peak, peak_kind = _peaks()
     achieved = bytes_per_launch / (mean[top] / 1e3) / 1e9
     traffic = None
@@ -333,7 +337,8 @@ def main():
         line = {
             "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if p.precision == 1 else "f64",
             "data": "synthetic seeded disk (no public dataset), one independent disk per GPU",
             "config": {"workload": desc, "cells": cells, "imax": p.imax, "jmax": p.jmax, "kmax": p.kmax,
                        "parallelism": f"replicas{ws}",

@@ -66,7 +66,8 @@ typedef struct pg_params {
   double noise_amp;       /* multiplicative Sigma noise amplitude (1e-4)      */
   double kill_rin;        /* wave damping for r < kill_rin (0 = none)         */
   double kill_rout;       /* wave damping for r > kill_rout (0 = none)        */
-  int    precision;       /* 0 = FP64 throughout                              */
+  int    precision;       /* 0 = FP64 throughout; 1 = FP32 planes, FP64
+                             geometry, forces, time step and reductions    */
   int    reserved[7];
 } pg_params;
 
@@ -219,10 +220,14 @@ int pg_advance_graph(pg_run *run, int nsteps, int chunk, int *taken);
 
 /* ---- device buffers (for harnesses that keep data resident) -------------- */
 typedef struct pg_device_view {
-  double *sigma, *vr, *vphi;  /* current planes, [imax*kmax][jmax] physical  */
+  void   *sigma, *vr, *vphi;  /* current planes, first interior ring of the
+                                 first polar layer, azimuth in physical order */
   int64_t row_stride;         /* elements between rings                      */
+  int64_t slab_stride;        /* elements between polar layers (3D)          */
   int    imax, jmax, kmax;
-  int    pad;
+  int    elem_bytes;          /* 8: double planes (precision 0); 4: float
+                                 planes (precision 1), where vphi holds
+                                 v_phi minus the ring's initial-state v_phi */
   void  *stream;              /* cudaStream_t the run launches on            */
 } pg_device_view;
 int pg_device_view_get(pg_run *run, pg_device_view *view);

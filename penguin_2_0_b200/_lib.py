@@ -77,8 +77,8 @@ class pg_clock(C.Structure):
 class pg_device_view(C.Structure):
     _fields_ = [
         ("sigma", C.c_void_p), ("vr", C.c_void_p), ("vphi", C.c_void_p),
-        ("row_stride", C.c_int64), ("imax", C.c_int), ("jmax", C.c_int), ("kmax", C.c_int),
-        ("pad", C.c_int), ("stream", C.c_void_p),
+        ("row_stride", C.c_int64), ("slab_stride", C.c_int64), ("imax", C.c_int), ("jmax", C.c_int), ("kmax", C.c_int),
+        ("elem_bytes", C.c_int), ("stream", C.c_void_p),
     ]
 
 

@@ -1,0 +1,420 @@
+// pg_chunk32.cuh -- the ppmlr chain in FP32 (the run's precision = 1).
+//
+// Same phases, index ranges and formulas as ppm_chunk (pg_chunk.cuh), with
+// these changes that keep FP32 accurate on a Keplerian disk:
+//  * Sigma is stored as the residual dS = Sigma - S_bg(ring) from the ring's
+//    initial-state density, and the kernels carry Sigma in FP64 per cell
+//    (CellIn32::sig): mass m = Sigma dvol and m + f_in - f_out are FP64 with
+//    FP32 fluxes, so a per-step change far below Sigma's FP32 spacing (the
+//    slow viscous evolution of the disk: ~4e-8 of Sigma per step) is kept
+//    instead of being rounded away every step;
+//  * azimuthal velocities are residuals dv = v_phi - v_bg(ring): the
+//    azimuthal sweep is exactly invariant under a per-ring shift of the
+//    velocity (PPM limiters and the isothermal Riemann solver only see
+//    differences), and the FARGO residual angular velocity
+//    v_bg/r - v_rot - FrRot is an FP64 per-ring constant;
+//  * the radial and polar sweeps carry the angular momentum
+//    L = r_cyl (v_bg + dv) in FP64 (slot L, its remap uses FP64 masses so
+//    that m_new = m + flux_in - flux_out is consistent to rounding); FP32
+//    would round L to 6e-8 of v_K, far above the disk's perturbations;
+//  * Lagrangian face positions are kept as displacements delx from the
+//    Eulerian faces (widths dx = dx0 + delx[n+1] - delx[n]), so FP32 does not
+//    lose the small face motions against face coordinates of order 1;
+//  * forces, geometry factors and positions are evaluated in FP64 from the
+//    FP64 face coordinate of each cell.
+#pragma once
+#include "pg_chunk.cuh"
+
+namespace pgd {
+
+constexpr float kSmallpF = 1.0e-15f;
+constexpr float kSmallrF = 1.0e-15f;
+constexpr float kFourthdF = 1.3333333333333333f;
+
+template <int NT>
+struct ChunkShm32 {
+  float r[NT + 2], p[NT + 2], u[NT + 2], v[NT + 2], w[NT + 2], dx0[NT + 2];
+  float q[NT + 2], dx[NT + 2], umid[NT + 2], pmid[NT + 2], tmp1[NT + 2], dl[NT + 2];
+  double L[NT + 2], Lal[NT + 2], Lda[NT + 2], La6[NT + 2], Lflux[NT + 2], xa0[NT + 2];
+};
+
+struct CellIn32 {
+  double rad, azi, pol, vrot, dvol0;
+  double omres;   // azimuthal sweep: v_bg / r_cyl - v_rot - FrRot (FP64)
+  double sig;     // this cell's Sigma in FP64 (S_bg + dS)
+};
+
+__device__ __forceinline__ float min3f(float A, float B, float C) {
+  if (A < B) { if (C < A) return C; else return A; }
+  else       { if (C < B) return C; else return B; }
+}
+__device__ __forceinline__ float max3f(float A, float B, float C) {
+  if (A > B) { if (C > A) return C; else return A; }
+  else       { if (C > B) return C; else return B; }
+}
+
+struct ParF { float c0, c1, c2, c3, c4; };
+
+__device__ __forceinline__ void paraset32(int n, int nmin, int nmax, ParF &par, const float *dx, float *a,
+                                          float *ai, float *b) {
+  float dx_n = 0.f, ain = 0.f, bi = 0.f, ci = 0.f, c = 0.f;
+  if (n >= nmin && n < nmax - 1) {
+    dx_n = dx[n];
+    float an = dx_n + dx[n + 1];
+    ain = 1.0f / an;
+    float bn = an + dx_n;
+    bi = 1.0f / bn;
+    c = an + dx[n + 1];
+    ci = 1.0f / c;
+    a[n] = an; ai[n] = ain; b[n] = bn;
+  }
+  __syncthreads();
+  if (n >= nmin + 1 && n < nmax - 2) {
+    float d = 1.0f / (a[n - 1] + a[n + 1]);
+    par.c0 = dx_n * ain * (1.0f + 2.0f * d * dx[n + 1] * (a[n - 1] * bi - a[n + 1] * ci));
+    par.c1 = -d * dx_n * a[n - 1] * bi;
+    par.c2 = d * dx[n + 1] * a[n + 1] * ci;
+  }
+  if (n >= nmin + 1 && n < nmax - 1) {
+    float d = dx_n / (a[n - 1] + dx[n + 1]);
+    par.c3 = d * b[n - 1] * ain;
+    par.c4 = d * c * ai[n - 1];
+  }
+  __syncthreads();
+}
+
+// parabola on values of type T (float, or double for the L slot) with FP32
+// coefficients
+template <typename T>
+__device__ __forceinline__ void parabola32(int n, int nmin, int nmax, float flat, const T *val, T *al, T *da,
+                                           T *a6, const ParF &par) {
+  T t1 = 0, a = 0, ar = 0, da_r = 0;
+  if (n >= nmin + 1 && n < nmax - 1) {
+    a = val[n];
+    da_r = val[n + 1] - a;
+    T da_l = a - val[n - 1];
+    t1 = (T)par.c3 * da_r + (T)par.c4 * da_l;
+    T two = 2;
+    T m1 = two * fabs(da_l), m2 = two * fabs(da_r);
+    if (t1 < 0) { T x = -t1; T mn = (x < m1) ? ((m2 < x) ? m2 : x) : ((m2 < m1) ? m2 : m1); t1 = -mn; }
+    else        { T x = t1;  T mn = (x < m1) ? ((m2 < x) ? m2 : x) : ((m2 < m1) ? m2 : m1); t1 = mn; }
+    if (da_l * da_r < 0) t1 = 0;
+    a6[n] = t1;
+  }
+  __syncthreads();
+  if (n >= nmin + 1 && n < nmax - 2) {
+    ar = a + (T)par.c0 * da_r + (T)par.c1 * a6[n + 1] + (T)par.c2 * t1;
+    al[n + 1] = ar;
+  }
+  __syncthreads();
+  if (n >= nmin + 2 && n < nmax - 2) {
+    T f = (T)flat;
+    T u1 = f * a;
+    T u2 = (T)1 - f;
+    T xr = u1 + u2 * ar;
+    T la = u1 + u2 * al[n];
+    u1 = xr - la;
+    u2 = u1 * u1;
+    T half = (T)0.5, six = (T)6, three = (T)3, two = (T)2;
+    u1 = u1 * (six * (a - half * (xr + la)));
+    if ((xr - a) * (a - la) <= 0) { xr = a; la = a; }
+    if (u2 < u1) la = three * a - two * xr;
+    if (u2 < -u1) xr = three * a - two * la;
+    da[n] = xr - la;
+    a6[n] = six * (a - half * (xr + la));
+    al[n] = la;
+  }
+  __syncthreads();
+}
+
+template <int AXIS, bool SPH>
+__device__ __forceinline__ double face_force32(int n, double hdt, const CellIn32 &c, double xa0f,
+                                               const double *Lv, const float *wv, const Body &pl,
+                                               const Phys &ph) {
+  // Lv: the FP64 angular-momentum slot (radial: v slot, polar: w slot);
+  // wv: the other transverse FP32 slot (radial 3D: w = r v_theta)
+  if (AXIS == 0) {
+    double rad = xa0f;
+    double azi = c.azi + hdt * c.vrot;
+    double grav;
+    if (!SPH) {
+      if (ph.plnt) { grav = grav_rad_cyl(rad, azi, c.pol, pl, hdt); grav += -1.0 / rad / rad; }
+      else { double dis = sqrt(rad * rad + c.pol * c.pol); grav = -rad / dis / dis / dis; }
+      double vf = 0.5 * (Lv[n] + Lv[n - 1]);
+      return grav + vf * vf / rad / rad / rad;
+    } else {
+      grav = ph.plnt ? grav_rad_sph(rad, azi, c.pol, pl, hdt) : -1.0 / rad / rad;
+      double wf = 0.5 * ((double)wv[n] + (double)wv[n - 1]);
+      double vf = 0.5 * (Lv[n] + Lv[n - 1]);
+      double rs = rad * sin(c.pol);
+      return grav + wf * wf / rad / rad / rad + vf * vf / rad / (rs * rs);
+    }
+  } else if (AXIS == 1) {
+    double azi = xa0f + hdt * c.vrot;
+    if (!SPH) return ph.plnt ? grav_azi_cyl(c.rad, azi, c.pol, pl, hdt) : 0.0;
+    return ph.plnt ? grav_azi_sph(c.rad, azi, c.pol, pl, hdt) : 0.0;
+  } else {
+    double pol = xa0f;
+    double azi = c.azi + hdt * c.vrot;
+    double grav = ph.plnt ? grav_pol_sph(c.rad, azi, pol, pl, hdt) : 0.0;
+    double rc = c.rad * sin(pol);
+    double lf = 0.5 * (Lv[n] + Lv[n - 1]);
+    return grav + (lf * lf * cos(pol)) / rc / rc / rc;
+  }
+}
+
+template <int AXIS, bool SPH>
+__device__ __forceinline__ double centre_force32(int n, double dt, double rad, double azi, double pol,
+                                                 const double *Lv, const float *wv, const Body &pl,
+                                                 const Phys &ph) {
+  if (AXIS == 0) {
+    double grav;
+    if (!SPH) {
+      if (ph.plnt) { grav = grav_rad_cyl(rad, azi, pol, pl, dt); grav += -1.0 / rad / rad; }
+      else { double dis = sqrt(rad * rad + pol * pol); grav = -rad / dis / dis / dis; }
+      return grav + Lv[n] * Lv[n] / rad / rad / rad;
+    } else {
+      grav = ph.plnt ? grav_rad_sph(rad, azi, pol, pl, dt) : -1.0 / rad / rad;
+      double w = wv[n];
+      double rs = rad * sin(pol);
+      return grav + w * w / rad / rad / rad + Lv[n] * Lv[n] / rad / (rs * rs);
+    }
+  } else if (AXIS == 1) {
+    if (!SPH) return ph.plnt ? grav_azi_cyl(rad, azi, pol, pl, dt) : 0.0;
+    return ph.plnt ? grav_azi_sph(rad, azi, pol, pl, dt) : 0.0;
+  } else {
+    double grav = ph.plnt ? grav_pol_sph(rad, azi, pol, pl, dt) : 0.0;
+    double rc = rad * sin(pol);
+    return grav + (Lv[n] * Lv[n] * cos(pol)) / rc / rc / rc;
+  }
+}
+
+// FP32 ppmlr chain; returns this cell's new Sigma in FP64 (cells 6 ..
+// nmax-7; the others return c.sig).  Slots: u = sweep velocity (FP32; residual dv_phi in
+// the azimuthal sweep); L = FP64 angular momentum (radial: the v slot,
+// polar: the w slot); the remaining transverse slot in FP32 (radial 3D: w,
+// azimuthal: w = v_r and in 3D v = v_theta, polar: v = v_r).  xa0 holds the
+// FP64 face coordinates.
+template <int AXIS, bool SPH, bool THREED, int NT>
+__device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax, double dt, double FrRot,
+                                            const CellIn32 &c, const Body &pl, const Phys &ph) {
+  const bool act = n < nmax;
+  const bool hasL = (AXIS != 1);
+  float flat = 0.f;
+  if (act) { S.q[n] = 0.f; S.dx[n] = 0.f; S.umid[n] = 0.f; S.pmid[n] = 0.f; S.tmp1[n] = 0.f; S.dl[n] = 0.f; }
+  __syncthreads();
+  if (ph.flat) {
+    float *steep = S.tmp1;
+    if (act) {
+      bool shock = false;
+      steep[n] = 0.f;
+      if (n >= 2 && n < nmax - 2) {
+        float dp1 = S.p[n + 1] - S.p[n - 1];
+        float dp2 = S.p[n + 2] - S.p[n - 2];
+        if (fabsf(dp2) < kSmallpF) dp2 = kSmallpF;
+        float ddp = fabsf(dp1) / fminf(S.p[n + 1], S.p[n - 1]);
+        if (ddp > 0.33f) shock = true;
+        if (S.u[n - 1] < S.u[n + 1]) shock = false;
+        if (shock) {
+          ddp = (dp1 / dp2 - 0.75f) * 5.0f;
+          steep[n] = fmaxf(0.f, ddp);
+        }
+      }
+    }
+    __syncthreads();
+    if (n >= 2 && n < nmax - 2) flat = fminf(0.5f, max3f(steep[n - 1], steep[n], steep[n + 1]));
+    __syncthreads();
+  }
+  // ---- states ----
+  const double hdt = 0.5 * dt;
+  const float hdtf = (float)hdt;
+  ParF par;
+  paraset32(n, 0, nmax, par, S.dx0, S.q, S.dx, S.tmp1);
+  float ftot = 0.f;
+  if (n >= 2 && n < nmax - 1) ftot = (float)face_force32<AXIS, SPH>(n, hdt, c, S.xa0[n], S.L, AXIS == 0 ? S.w : S.v, pl, ph);
+  __syncthreads();
+  if (act) {
+    float cs = hdtf * sqrtf(ph.gam * S.p[n] / S.r[n]) / S.dx0[n];
+    if (AXIS != 0) cs /= (float)c.rad;
+    S.umid[n] = cs;
+    S.pmid[n] = 1.0f - kFourthdF * cs;
+  }
+  float spl = 0.f, spr = 0.f, srl = 0.f, srr = 0.f, sul = 0.f, sur = 0.f;
+  const float *cs = S.umid, *csfac = S.pmid;
+  float *al = S.q, *da = S.dx, *a6 = S.tmp1;
+  parabola32<float>(n, 0, nmax, flat, S.p, al, da, a6, par);
+  if (n >= 3 && n < nmax - 2) {
+    float t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
+    spl = fmaxf(kSmallpF, t);
+    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
+    spr = fmaxf(kSmallpF, t);
+  }
+  __syncthreads();
+  parabola32<float>(n, 0, nmax, flat, S.r, al, da, a6, par);
+  if (n >= 3 && n < nmax - 2) {
+    float t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
+    srl = fmaxf(kSmallrF, t);
+    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
+    srr = fmaxf(kSmallrF, t);
+  }
+  __syncthreads();
+  parabola32<float>(n, 0, nmax, flat, S.u, al, da, a6, par);
+  if (n >= 3 && n < nmax - 2) {
+    float t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
+    sul = t + hdtf * ftot;
+    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
+    sur = t + hdtf * ftot;
+  }
+  __syncthreads();
+  // ---- riemann (isothermal) ----
+  if (n >= 3 && n < nmax - 2) {
+    float t1 = 0.5f * (sqrtf(spl / srl) + sqrtf(spr / srr));
+    float t2 = -0.5f * (sur - sul) / t1;
+    float pm = sqrtf(spl * spr) * expf(t2);
+    S.umid[n] = sul - t1 * logf(pm / spl);
+    S.pmid[n] = fmaxf(kSmallpF, pm);
+  }
+  __syncthreads();
+  // ---- evolve: face displacements delx (dl), widths dx0 + dl[n+1] - dl[n] ----
+  float *vfac = S.tmp1;
+  const double xa0n = act ? S.xa0[n] : 0.0;
+  double dvol = c.dvol0;
+  float dtdm = 0.f, fto1 = 0.f, fto2 = 0.f;
+  if (n >= 3 && n < nmax - 2) {
+    double delx;
+    if (AXIS == 0) delx = dt * (double)S.umid[n];
+    else if (AXIS == 1) delx = dt * ((double)S.umid[n] / c.rad + c.omres);
+    else delx = dt * (double)S.umid[n] / c.rad;
+    dtdm = (float)(dt / ((double)S.r[n] * c.dvol0));
+    S.dl[n] = (float)delx;
+  }
+  __syncthreads();
+  double xa = xa0n;
+  float dxl = 0.f;
+  if (n >= 3 && n < nmax - 3) {
+    dxl = S.dx0[n] + (S.dl[n + 1] - S.dl[n]);
+    S.dx[n] = dxl;
+    xa = xa0n + (double)S.dl[n];
+  }
+  __syncthreads();
+  if (n >= 3 && n < nmax - 3) {
+    double xcl = xa + 0.5 * (double)dxl;
+    double a1, a2;
+    if (AXIS == 0) {
+      a1 = centre_force32<0, SPH>(n, 0.0, c.rad, c.azi, c.pol, S.L, S.w, pl, ph);
+      a2 = centre_force32<0, SPH>(n, dt, xcl, c.azi + dt * c.vrot, c.pol, S.L, S.w, pl, ph);
+    } else if (AXIS == 1) {
+      a1 = centre_force32<1, SPH>(n, 0.0, c.rad, c.azi, c.pol, S.L, S.v, pl, ph);
+      a2 = centre_force32<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, S.L, S.v, pl, ph);
+    } else {
+      a1 = centre_force32<2, SPH>(n, 0.0, c.rad, c.azi, c.pol, S.L, S.v, pl, ph);
+      a2 = centre_force32<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, S.L, S.v, pl, ph);
+    }
+    fto1 = (float)a1;
+    fto2 = (float)a2;
+  }
+  __syncthreads();
+  if (n >= 3 && n < nmax - 2) {
+    // as in the reference, the last cell of this range keeps xa = xa0
+    // (evolve.cu:36-44 sets xa for n < nmax-3 only)
+    double dxn = S.dx[n];
+    double d = (n < nmax - 3) ? (double)S.dl[n] : 0.0;
+    if (AXIS == 0) {
+      if (!SPH) { dvol = dxn * (xa + 0.5 * dxn); vfac[n] = (float)(xa0n + 0.5 * d); }
+      else {
+        dvol = dxn * (xa * (xa + dxn) + dxn * dxn * kThird);
+        vfac[n] = (float)(d * (kThird * d + xa0n) + (xa0n * xa0n));
+      }
+    } else if (AXIS == 1) {
+      dvol = dxn * c.rad; vfac[n] = 1.0f;
+    } else {
+      dvol = 2.0 * sin(xa + 0.5 * dxn) * sin(0.5 * dxn) * c.rad;
+      if (d == 0.0) vfac[n] = (float)sin(xa);
+      else vfac[n] = (float)(2.0 * sin(xa0n + 0.5 * d) * sin(0.5 * d) / d);
+    }
+  }
+  __syncthreads();
+  double m_d = 0.0;
+  if (n >= 3 && n < nmax - 3) {
+    double rl = c.sig * (c.dvol0 / dvol);
+    m_d = c.sig * c.dvol0;   // Lagrangian mass, FP64
+    S.r[n] = fmaxf((float)rl, kSmallrF);
+    float dum = S.u[n];
+    float delx = 0.5f * (float)dt * (fto1 + fto2);
+    delx += -dtdm * (S.pmid[n + 1] - S.pmid[n]) * 0.5f * (vfac[n + 1] + vfac[n]);
+    S.u[n] = dum + delx;
+  }
+  __syncthreads();
+  // ---- remap ----
+  al = S.tmp1; da = S.umid; a6 = S.pmid;
+  paraset32(n, 3, nmax - 3, par, S.dx, al, da, a6);
+  double dd = (n >= 3 && n < nmax - 3) ? (double)S.dl[n] : 0.0;
+  double lvol;
+  if (AXIS == 0) {
+    if (!SPH) lvol = dd * (xa0n + 0.5 * dd);
+    else lvol = dd * (xa0n * (xa0n + dd) + kThird * (dd * dd));
+  } else if (AXIS == 1) {
+    lvol = dd * c.rad;
+  } else {
+    lvol = 2.0 * sin(xa0n + 0.5 * dd) * sin(0.5 * dd) * c.rad;
+  }
+  float dxf = (float)dd;
+  const bool delC = (dxf >= 0.f);
+  parabola32<float>(n, 3, nmax - 3, flat, S.r, al, da, a6, par);
+  float *flux = S.dx;
+  float dxnn = 0.f, dxnm = 0.f;
+  if (n >= 6 && n < nmax - 5) { dxnn = S.dx[n]; dxnm = S.dx[n - 1]; }
+  __syncthreads();
+  float dxf2 = 0.f, fr = 0.f;
+  if (n >= 6 && n < nmax - 5) {
+    if (delC) {
+      dxf = 0.5f * dxf / dxnm;
+      dxf2 = 1.0f - kFourthdF * dxf;
+      fr = (al[n - 1] + da[n - 1] - dxf * (da[n - 1] - dxf2 * a6[n - 1])) * (float)lvol;
+    } else {
+      dxf = 0.5f * dxf / dxnn;
+      dxf2 = 1.0f + kFourthdF * dxf;
+      fr = (al[n] - dxf * (da[n] + dxf2 * a6[n])) * (float)lvol;
+    }
+    flux[n] = fr;
+  }
+  __syncthreads();
+  float mm = 0.f, invm = 0.f;
+  double mnew_d = 1.0, sig_new = c.sig;
+  if (n >= 6 && n < nmax - 6) {
+    mm = S.r[n] * (float)dvol;
+    mnew_d = m_d + (double)fr - (double)flux[n + 1];
+    sig_new = fmax((double)kSmallrF, mnew_d / c.dvol0);
+    S.r[n] = (float)sig_new;
+    invm = 1.0f / (S.r[n] * (float)c.dvol0);
+  }
+  auto remap_f = [&](float *fld) {
+    parabola32<float>(n, 3, nmax - 3, flat, fld, al, da, a6, par);
+    if (n >= 6 && n < nmax - 5) {
+      if (delC) flux[n] = (al[n - 1] + da[n - 1] - dxf * (da[n - 1] - dxf2 * a6[n - 1])) * fr;
+      else      flux[n] = (al[n] - dxf * (da[n] + dxf2 * a6[n])) * fr;
+    }
+    __syncthreads();
+    if (n >= 6 && n < nmax - 6) fld[n] = (fld[n] * mm + (flux[n] - flux[n + 1])) * invm;
+  };
+  remap_f(S.u);
+  if (hasL) {
+    // FP64 angular momentum: L_new = (L m + F_n - F_{n+1}) / (m + f_n - f_{n+1})
+    parabola32<double>(n, 3, nmax - 3, flat, S.L, S.Lal, S.Lda, S.La6, par);
+    if (n >= 6 && n < nmax - 5) {
+      double x = dxf, x2 = dxf2;
+      if (delC) S.Lflux[n] = (S.Lal[n - 1] + S.Lda[n - 1] - x * (S.Lda[n - 1] - x2 * S.La6[n - 1])) * (double)fr;
+      else      S.Lflux[n] = (S.Lal[n] - x * (S.Lda[n] + x2 * S.La6[n])) * (double)fr;
+    }
+    __syncthreads();
+    if (n >= 6 && n < nmax - 6) S.L[n] = (S.L[n] * m_d + (S.Lflux[n] - S.Lflux[n + 1])) / mnew_d;
+    __syncthreads();
+  }
+  if (AXIS == 0) { if (THREED) remap_f(S.w); }
+  else if (AXIS == 1) { remap_f(S.w); if (THREED) remap_f(S.v); }
+  else remap_f(S.v);
+  __syncthreads();
+  return sig_new;
+}
+
+}  // namespace pgd

@@ -248,8 +248,8 @@ int config_params(int which, pg_params *p) {
       p->nudr = 3; p->ntop = 0;  // fixed upper layers, reflecting midplane
       p->endtime = 5.0 * kTwoPi; p->tmovie = p->endtime;
       return PG_OK;
-    case 2:  // 1024 x 3072, same disk and planet as the 256 x 768 case, 20 orbits
-      p->imax = 1024; p->jmax = 3072; p->kmax = 1; p->ndim = 2;
+    case 2:  // 1024 x 3072 FP32 planes, same disk and planet as the 256 x 768 case, 20 orbits
+      p->imax = 1024; p->jmax = 3072; p->kmax = 1; p->ndim = 2; p->precision = 1;
       p->xmin = 0.4; p->xmax = 2.5; p->kill_rin = 0.5; p->kill_rout = 2.2;
       p->endtime = 20.0 * kTwoPi; p->tmovie = p->endtime;
       return PG_OK;

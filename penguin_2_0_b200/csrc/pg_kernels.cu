@@ -608,7 +608,8 @@ __device__ __forceinline__ double tree1024(double *list) {
   return list[0];
 }
 
-__global__ void __launch_bounds__(1024) k_reduce(Tables T, const double *R, Body pl, const DevClock *clk,
+template <typename RT>
+__global__ void __launch_bounds__(1024) k_reduce(Tables T, const RT *R, Body pl, const DevClock *clk,
                                                  double exclude, int mode, int plnt, double p_alpha,
                                                  int ndim, double *ring_part, unsigned int *counter,
                                                  double *out, double *hist_row) {
@@ -626,6 +627,8 @@ __global__ void __launch_bounds__(1024) k_reduce(Tables T, const double *R, Body
   const int rot = T.rot_j[rk];
   const double rad = T.rxc[row], xvol = T.rxvol[row];
   const double zvol = (ndim == 3) ? T.zvol[k + NPAD] : 1.0;
+  // FP32 planes hold Sigma - S_bg(ring)
+  const double r_off = (sizeof(RT) == 4) ? T.sbg[rk] : 0.0;
   const int loop = nphi / 1024 + (nphi % 1024 != 0);
   double val = 0.0;
   for (int l = 0; l < loop; l++) {
@@ -634,7 +637,7 @@ __global__ void __launch_bounds__(1024) k_reduce(Tables T, const double *R, Body
     if (j < nphi) {
       int j0 = wrap1(j + rot, nphi);
       double phi = T.yc[j0];
-      double r = R[base + j0];
+      double r = r_off + (double)R[base + j0];
       if (plnt) {
         if (mode == 0) v = r * xvol * T.yvol[j0] * zvol;
         else if (ndim == 2 && (mode == 8 || mode == 9)) {
@@ -963,8 +966,16 @@ void reduce(const Tables &T, const double *r, const Body &pl, const DevClock *cl
             int mode, int plnt, double p_alpha, int ndim, double *ring_part, unsigned int *counter,
             double *out, double *hist_row, cudaStream_t s) {
   dim3 grid(T.nr, T.nk);
-  k_reduce<<<grid, 1024, 0, s>>>(T, r, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter,
-                                 out, hist_row);
+  k_reduce<double><<<grid, 1024, 0, s>>>(T, r, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter,
+                                         out, hist_row);
+}
+
+void reduce32(const Tables &T, const float *r, const Body &pl, const DevClock *clk, double exclude, int mode,
+              int plnt, double p_alpha, int ndim, double *ring_part, unsigned int *counter, double *out,
+              cudaStream_t s) {
+  dim3 grid(T.nr, T.nk);
+  k_reduce<float><<<grid, 1024, 0, s>>>(T, r, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter,
+                                        out, nullptr);
 }
 
 void prestep(DevClock *clk, const Tables &T, int fargo, cudaStream_t s) {

@@ -37,6 +37,8 @@ struct Tables {
   const double *val_r, *val_u, *val_v;          // [nk*nrg] damping / FARGO targets
   const double *damp_g, *damp_pw;               // [nk*nrg] zone factor, r^-1.5
   const double *tg;                             // [6*nr*4] theta ghost state (udr): r,p,u,v
+  const double *vbg;                            // [nk*nrg] FP32 runs: v_phi background (val.v / ghost v)
+  const double *sbg;                            // [nk*nrg] FP32 runs: Sigma background (val.r / ghost r)
   double *res_v, *rot_v;                        // [nk*nrg]
   int *inc_j, *rot_j;                           // [nk*nrg]
 };
@@ -45,6 +47,12 @@ struct Planes {
   const double *r, *u, *v, *w;
   double *ro, *uo, *vo, *wo;
   const double *p0;   // non-null: pressure of a freshly loaded dump (first sweep only)
+};
+
+// FP32 planes: dS = Sigma - S_bg, v_r, dv = v_phi - v_bg, v_theta
+struct Planes32 {
+  const float *r, *u, *v, *w;
+  float *ro, *uo, *vo, *wo;
 };
 
 // The device-resident clock of the fused loop (main.cu:270-441).
@@ -93,6 +101,17 @@ void damp(const Tables &T, double *r, double *u, double *v, double *w, double dt
 void reduce(const Tables &T, const double *r, const Body &pl, const DevClock *clk, double exclude,
             int mode, int plnt, double p_alpha, int ndim, double *ring_part, unsigned int *counter,
             double *out, double *hist_row, cudaStream_t s);
+void reduce32(const Tables &T, const float *r, const Body &pl, const DevClock *clk, double exclude, int mode,
+              int plnt, double p_alpha, int ndim, double *ring_part, unsigned int *counter, double *out,
+              cudaStream_t s);
+// FP32 sweeps (pg_kernels32.cu)
+void sweep_x32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s);
+void sweep_y32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s);
+void sweep_z32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s);
+void cfl32(const Tables &T, const Planes32 &cur, const Phys &ph, double frrot, int ndim, int rot_pending,
+           unsigned long long *out, int *status, cudaStream_t s);
+void damp32(const Tables &T, const Planes32 &cur, double dt, const DevClock *clk, int ndim, cudaStream_t s);
+void cfl32_clk(const Tables &T, const Planes32 &cur, const Phys &ph, int ndim, DevClock *clk, cudaStream_t s);
 void damp_clk(const Tables &T, double *r, double *u, double *v, double *w, const DevClock *clk,
               cudaStream_t s);
 void cfl_clk(const Tables &T, const double *r, const double *u, const double *v, const double *w,

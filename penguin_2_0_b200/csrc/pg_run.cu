@@ -34,6 +34,10 @@ struct pg_run {
   int nr = 0, nphi = 0, nk = 0, nrg = 0;
   size_t plane_elems = 0;
   double *planes[2][4] = {{nullptr}};
+  float *p32[2][4] = {{nullptr}};      // precision 1: Sigma, v_r, dv_phi, v_theta in FP32
+  bool fp32 = false;
+  double *vbg = nullptr;   // [nk*nrg] v_phi background of each ring row (FP32 runs)
+  double *sbg = nullptr;   // [nk*nrg] Sigma background of each ring row (FP32 runs)
   double *p0 = nullptr;
   bool p0_live = false;
   int cur = 0;
@@ -53,6 +57,7 @@ struct pg_run {
   int hist_cap = 4096;
   // host side
   std::vector<unsigned char> tmpl;   // last loaded dump (geometry fields)
+  std::vector<double> h_vbg, h_sbg;
   std::vector<double> h_cs2;
   bool loaded = false;
   bool clock_ready = false;
@@ -61,6 +66,10 @@ struct pg_run {
   cudaGraphExec_t gexec = nullptr;
   int gsteps = 0;
   int64_t graph_kernels = 0;       // kernels per replay of gexec
+  // early exit of pg_advance*: pinned copies of clk->halted, read a few
+  // launches behind the one being queued
+  int *h_halt = nullptr;
+  cudaEvent_t halt_ev[4] = {};
   // event timing
   bool timing = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -110,6 +119,22 @@ static int check_launch(pg_run *run, int n) {
   return PG_OK;
 }
 
+static pgd::Planes32 planes32_fwd(pg_run *run, int src) {
+  pgd::Planes32 p;
+  p.r = run->p32[src][0]; p.u = run->p32[src][1]; p.v = run->p32[src][2]; p.w = run->p32[src][3];
+  p.ro = run->p32[1 - src][0]; p.uo = run->p32[1 - src][1]; p.vo = run->p32[1 - src][2];
+  p.wo = run->p32[1 - src][3];
+  return p;
+}
+// the current FP32 planes as both source and target (in-place kernels)
+static pgd::Planes32 planes32_cur(pg_run *run) {
+  pgd::Planes32 p;
+  int c = run->cur;
+  p.r = p.ro = run->p32[c][0]; p.u = p.uo = run->p32[c][1]; p.v = p.vo = run->p32[c][2];
+  p.w = p.wo = run->p32[c][3];
+  return p;
+}
+
 static pgd::Planes planes_fwd(pg_run *run, int src, const double *p0) {
   pgd::Planes p;
   p.r = run->planes[src][0]; p.u = run->planes[src][1]; p.v = run->planes[src][2]; p.w = run->planes[src][3];
@@ -142,11 +167,17 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
   if (cudaSetDevice(device) != cudaSuccess) { delete run; return PG_ERR_CUDA; }
   if (cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PG_ERR_CUDA);
   run->plane_elems = (size_t)run->nk * run->nrg * run->nphi;
+  run->fp32 = (p->precision == 1);
   int nf = (p->ndim == 3) ? 4 : 3;
   for (int b = 0; b < 2; b++)
-    for (int f = 0; f < nf; f++)
-      if (cudaMalloc(&run->planes[b][f], run->plane_elems * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
-  if (cudaMalloc(&run->p0, run->plane_elems * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+    for (int f = 0; f < nf; f++) {
+      if (run->fp32) {
+        if (cudaMalloc(&run->p32[b][f], run->plane_elems * sizeof(float)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+      } else {
+        if (cudaMalloc(&run->planes[b][f], run->plane_elems * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+      }
+    }
+  if (!run->fp32 && cudaMalloc(&run->p0, run->plane_elems * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
   // double tables
   int nrg = run->nrg, nphi = run->nphi, nk = run->nk, nr = run->nr;
   size_t nring = (size_t)nk * nrg;
@@ -176,6 +207,10 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
   T.z = t; t += nz; T.dz = t; t += nz; T.zvol = t; t += nz; T.zc = t; t += nz;
   T.tg = t; t += (size_t)2 * NPAD * nr * 4;
   if (cudaMalloc(&T.rot_v, nring * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  if (cudaMalloc(&run->vbg, nring * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  T.vbg = run->vbg;
+  if (cudaMalloc(&run->sbg, nring * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
+  T.sbg = run->sbg;
 
   T.inc_j = run->itab; T.rot_j = run->itab + nring;
   // scratch
@@ -205,8 +240,14 @@ int pg_destroy(pg_run *run) {
   if (run->stream) cudaStreamSynchronize(run->stream);
   if (run->gexec) cudaGraphExecDestroy(run->gexec);
   for (auto e : run->ev_pool) cudaEventDestroy(e);
+  for (auto e : run->halt_ev) if (e) cudaEventDestroy(e);
+  if (run->h_halt) cudaFreeHost(run->h_halt);
   for (auto &b : run->planes)
     for (auto &f : b) if (f) cudaFree(f);
+  for (auto &b : run->p32)
+    for (auto &f : b) if (f) cudaFree(f);
+  cudaFree(run->vbg);
+  cudaFree(run->sbg);
   cudaFree(run->p0);
   cudaFree(run->tab);
   cudaFree(run->itab);
@@ -250,7 +291,7 @@ int pg_load_rings(pg_run *run, const void *rings, size_t bytes) {
   // host images of the tables
   std::vector<double> rx(nrg), rdx(nrg), rxvol(nrg), rxc(nrg);
   std::vector<double> gp(nring, 0.0), vr(nring, 0.0), vu(nring, 0.0), vv(nring, 0.0);
-  std::vector<double> res_v(nring, 0.0), rot_v(nring, 0.0);
+  std::vector<double> res_v(nring, 0.0), rot_v(nring, 0.0), vbg(nring, 0.0), sbg(nring, 0.0);
   std::vector<int> inc_j(nring, 0), rot_j(nring, 0);
   std::vector<double> z(nz, 0.0), dz(nz, 0.0), zvol(nz, 0.0), zc(nz, 0.0);
   std::vector<double> tg((size_t)2 * NPAD * nr * 4, 0.0);
@@ -275,8 +316,8 @@ int pg_load_rings(pg_run *run, const void *rings, size_t bytes) {
   for (int k = 0; k < nk; k++) {
     for (int i = 0; i < NPAD; i++) {
       size_t a = (size_t)k * nrg + i, c = (size_t)k * nrg + nr + NPAD + i;
-      gp[a] = lft[i + NPAD * k].p; rot_v[a] = lft[i + NPAD * k].rot_v;
-      gp[c] = rgh[i + NPAD * k].p; rot_v[c] = rgh[i + NPAD * k].rot_v;
+      gp[a] = lft[i + NPAD * k].p; rot_v[a] = lft[i + NPAD * k].rot_v; vbg[a] = lft[i + NPAD * k].v; sbg[a] = lft[i + NPAD * k].r;
+      gp[c] = rgh[i + NPAD * k].p; rot_v[c] = rgh[i + NPAD * k].rot_v; vbg[c] = rgh[i + NPAD * k].v; sbg[c] = rgh[i + NPAD * k].r;
     }
     for (int i = 0; i < nr; i++) {
       size_t rk = (size_t)k * nrg + i + NPAD;
@@ -285,7 +326,7 @@ int pg_load_rings(pg_run *run, const void *rings, size_t bytes) {
       rot_j[rk] = *rv.rj(0); inc_j[rk] = *rv.rj(1);
       if (rot_j[rk] < 0 || rot_j[rk] >= nphi) return fail(run, PG_ERR_STATE, "rot_j out of range in dump");
       const pg::SymDisk &sv = val[i + (size_t)nr * k];
-      vr[rk] = sv.r; vu[rk] = sv.u; vv[rk] = sv.v;
+      vr[rk] = sv.r; vu[rk] = sv.u; vv[rk] = sv.v; vbg[rk] = sv.v; sbg[rk] = sv.r;
     }
   }
   // polar layers: lower ghosts (udr geometry), interior, upper ghosts (top geometry)
@@ -353,28 +394,50 @@ int pg_load_rings(pg_run *run, const void *rings, size_t bytes) {
   };
   CK(up(T.rx, rx)); CK(up(T.rdx, rdx)); CK(up(T.rxvol, rxvol)); CK(up(T.rxc, rxc));
   CK(up(T.gp, gp)); CK(up(T.val_r, vr)); CK(up(T.val_u, vu)); CK(up(T.val_v, vv));
-  CK(up(T.res_v, res_v)); CK(up(T.rot_v, rot_v));
+  CK(up(T.res_v, res_v)); CK(up(T.rot_v, rot_v)); CK(up(T.vbg, vbg)); CK(up(T.sbg, sbg));
   CK(cudaMemcpyAsync(T.inc_j, inc_j.data(), nring * sizeof(int), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(T.rot_j, rot_j.data(), nring * sizeof(int), cudaMemcpyHostToDevice, s));
   CK(up(T.y, g.zya)); CK(up(T.dy, g.zdy)); CK(up(T.yvol, g.yvol)); CK(up(T.yc, g.zyc));
   CK(up(T.z, z)); CK(up(T.dz, dz)); CK(up(T.zvol, zvol)); CK(up(T.zc, zc));
   CK(up(T.tg, tg));
-  for (int bsel = 0; bsel < 2; bsel++) {
-    CK(cudaMemcpyAsync(run->planes[bsel][0], hr.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(run->planes[bsel][1], hu.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(run->planes[bsel][2], hv.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
-    if (P.ndim == 3)
-      CK(cudaMemcpyAsync(run->planes[bsel][3], hw.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+  std::vector<float> fr, fu, fv, fw;
+  if (run->fp32) {
+    // FP32 planes: Sigma, v_r, dv = v_phi - v_bg(ring), v_theta
+    fr.resize(pe); fu.resize(pe); fv.resize(pe);
+    if (P.ndim == 3) fw.resize(pe);
+    for (size_t rkq = 0; rkq < nring; rkq++)
+      for (int j = 0; j < nphi; j++) {
+        size_t q = rkq * nphi + j;
+        fr[q] = (float)(hr[q] - sbg[rkq]); fu[q] = (float)hu[q]; fv[q] = (float)(hv[q] - vbg[rkq]);
+        if (P.ndim == 3) fw[q] = (float)hw[q];
+      }
+    for (int bsel = 0; bsel < 2; bsel++) {
+      CK(cudaMemcpyAsync(run->p32[bsel][0], fr.data(), pe * sizeof(float), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(run->p32[bsel][1], fu.data(), pe * sizeof(float), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(run->p32[bsel][2], fv.data(), pe * sizeof(float), cudaMemcpyHostToDevice, s));
+      if (P.ndim == 3)
+        CK(cudaMemcpyAsync(run->p32[bsel][3], fw.data(), pe * sizeof(float), cudaMemcpyHostToDevice, s));
+    }
+  } else {
+    for (int bsel = 0; bsel < 2; bsel++) {
+      CK(cudaMemcpyAsync(run->planes[bsel][0], hr.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(run->planes[bsel][1], hu.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(run->planes[bsel][2], hv.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+      if (P.ndim == 3)
+        CK(cudaMemcpyAsync(run->planes[bsel][3], hw.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    CK(cudaMemcpyAsync(run->p0, hp.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
   }
-  CK(cudaMemcpyAsync(run->p0, hp.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
   pgk::tables(T, run->ph, P.ndim, P.kill_rin, P.kill_rout, P.xmin, P.xmax, s);
   if (int e = check_launch(run, 1)) return e;
   CK(cudaStreamSynchronize(s));
   run->h_cs2.resize(nring);
   CK(cudaMemcpy(run->h_cs2.data(), T.cs2, nring * sizeof(double), cudaMemcpyDeviceToHost));
+  run->h_vbg = vbg;
+  run->h_sbg = sbg;
   run->tmpl.assign(b, b + bytes);
   run->cur = 0;
-  run->p0_live = true;
+  run->p0_live = !run->fp32;
   run->loaded = true;
   run->clock_ready = false;
   if (run->gexec) { cudaGraphExecDestroy(run->gexec); run->gexec = nullptr; run->gsteps = 0; }
@@ -407,11 +470,22 @@ int pg_save_rings(pg_run *run, void *rings, size_t bytes) {
   std::vector<double> res_v(nring), rot_v(nring);
   std::vector<int> inc_j(nring), rot_j(nring);
   cudaStream_t s = run->stream;
-  double **cp = run->planes[run->cur];
-  CK(cudaMemcpyAsync(hr.data(), cp[0], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(hu.data(), cp[1], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(hv.data(), cp[2], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
-  if (P.ndim == 3) CK(cudaMemcpyAsync(hw.data(), cp[3], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+  std::vector<float> fr, fu, fv, fw;
+  if (run->fp32) {
+    float **fp = run->p32[run->cur];
+    fr.resize(pe); fu.resize(pe); fv.resize(pe);
+    if (P.ndim == 3) fw.resize(pe);
+    CK(cudaMemcpyAsync(fr.data(), fp[0], pe * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(fu.data(), fp[1], pe * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(fv.data(), fp[2], pe * sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (P.ndim == 3) CK(cudaMemcpyAsync(fw.data(), fp[3], pe * sizeof(float), cudaMemcpyDeviceToHost, s));
+  } else {
+    double **cp = run->planes[run->cur];
+    CK(cudaMemcpyAsync(hr.data(), cp[0], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hu.data(), cp[1], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hv.data(), cp[2], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (P.ndim == 3) CK(cudaMemcpyAsync(hw.data(), cp[3], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
   if (run->p0_live) {
     hp.resize(pe);
     CK(cudaMemcpyAsync(hp.data(), run->p0, pe * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -421,6 +495,14 @@ int pg_save_rings(pg_run *run, void *rings, size_t bytes) {
   CK(cudaMemcpyAsync(inc_j.data(), run->T.inc_j, nring * sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(rot_j.data(), run->T.rot_j, nring * sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  if (run->fp32) {
+    for (size_t rkq = 0; rkq < nring; rkq++)
+      for (int j = 0; j < nphi; j++) {
+        size_t q = rkq * nphi + j;
+        hr[q] = run->h_sbg[rkq] + (double)fr[q]; hu[q] = fu[q]; hv[q] = run->h_vbg[rkq] + (double)fv[q];
+        if (P.ndim == 3) hw[q] = fw[q];
+      }
+  }
   unsigned char *out = (unsigned char *)rings;
   std::memcpy(out, run->tmpl.data(), bytes);
   for (int k = 0; k < nk; k++)
@@ -460,13 +542,22 @@ int pg_save_dump(pg_run *run, const char *path) {
 
 int pg_device_view_get(pg_run *run, pg_device_view *v) {
   if (!run || !v) return PG_ERR_ARG;
-  double **cp = run->planes[run->cur];
-  v->sigma = cp[0] + (size_t)NPAD * run->nphi;
-  v->vr = cp[1] + (size_t)NPAD * run->nphi;
-  v->vphi = cp[2] + (size_t)NPAD * run->nphi;
+  if (run->fp32) {
+    float **fp = run->p32[run->cur];
+    v->sigma = fp[0] + (size_t)NPAD * run->nphi;
+    v->vr = fp[1] + (size_t)NPAD * run->nphi;
+    v->vphi = fp[2] + (size_t)NPAD * run->nphi;
+    v->elem_bytes = 4;
+  } else {
+    v->elem_bytes = 8;
+    double **cp = run->planes[run->cur];
+    v->sigma = cp[0] + (size_t)NPAD * run->nphi;
+    v->vr = cp[1] + (size_t)NPAD * run->nphi;
+    v->vphi = cp[2] + (size_t)NPAD * run->nphi;
+  }
   v->row_stride = run->nphi;
+  v->slab_stride = (int64_t)run->nrg * run->nphi;
   v->imax = run->nr; v->jmax = run->nphi; v->kmax = run->nk;
-  v->pad = run->nrg;
   v->stream = (void *)run->stream;
   return PG_OK;
 }
@@ -479,8 +570,11 @@ int pg_get_dt(pg_run *run, double dt_old, double frrot, double *dt_out) {
   cudaStream_t s = run->stream;
   double **cp = run->planes[run->cur];
   CK(cudaMemsetAsync(run->cfl, 0, sizeof(unsigned long long), s));
-  pgk::cfl_full(run->T, cp[0], cp[1], cp[2], cp[3], run->p0_live ? run->p0 : nullptr, run->ph, frrot,
-                run->P.ndim, run->cfl, s);
+  if (run->fp32)
+    pgk::cfl32(run->T, planes32_cur(run), run->ph, frrot, run->P.ndim, 0, run->cfl, nullptr, s);
+  else
+    pgk::cfl_full(run->T, cp[0], cp[1], cp[2], cp[3], run->p0_live ? run->p0 : nullptr, run->ph, frrot,
+                  run->P.ndim, run->cfl, s);
   if (int e = check_launch(run, 1)) return e;
   unsigned long long bits = 0;
   CK(cudaMemcpyAsync(&bits, run->cfl, sizeof(bits), cudaMemcpyDeviceToHost, s));
@@ -525,9 +619,15 @@ int pg_sweep2d(pg_run *run, double dt, const pg_body *planet, double frrot) {
   CK(cudaSetDevice(run->dev));
   pgd::SweepCtl c = host_ctl(dt, planet, frrot);
   cudaStream_t s = run->stream;
-  pgk::sweep_x(run->T, planes_fwd(run, run->cur, run->p0_live ? run->p0 : nullptr), run->ph, c, 2, s);
-  c.shift = 1;
-  pgk::sweep_y(run->T, planes_fwd(run, 1 - run->cur, nullptr), run->ph, c, 2, s);
+  if (run->fp32) {
+    pgk::sweep_x32(run->T, planes32_fwd(run, run->cur), run->ph, c, 2, s);
+    c.shift = 1;
+    pgk::sweep_y32(run->T, planes32_fwd(run, 1 - run->cur), run->ph, c, 2, s);
+  } else {
+    pgk::sweep_x(run->T, planes_fwd(run, run->cur, run->p0_live ? run->p0 : nullptr), run->ph, c, 2, s);
+    c.shift = 1;
+    pgk::sweep_y(run->T, planes_fwd(run, 1 - run->cur, nullptr), run->ph, c, 2, s);
+  }
   if (run->P.FARGO_flag > 0) pgk::rotate(run->T, nullptr, s);
   run->p0_live = false;
   return check_launch(run, nx(run) + ny(run) + (run->P.FARGO_flag > 0 ? 1 : 0));
@@ -541,10 +641,17 @@ int pg_sweep3d(pg_run *run, double dt, const pg_body *planet, double frrot) {
   pgd::SweepCtl c = host_ctl(dt, planet, frrot);
   cudaStream_t s = run->stream;
   int a = run->cur;
-  pgk::sweep_x(run->T, planes_fwd(run, a, run->p0_live ? run->p0 : nullptr), run->ph, c, 3, s);
-  pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 3, s);
-  c.shift = 1;   // the polar sweep is the last one: it applies the FARGO shift
-  pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, run->P.ntop, s);
+  if (run->fp32) {
+    pgk::sweep_x32(run->T, planes32_fwd(run, a), run->ph, c, 3, s);
+    pgk::sweep_y32(run->T, planes32_fwd(run, 1 - a), run->ph, c, 3, s);
+    c.shift = 1;
+    pgk::sweep_z32(run->T, planes32_fwd(run, a), run->ph, c, run->P.ntop, s);
+  } else {
+    pgk::sweep_x(run->T, planes_fwd(run, a, run->p0_live ? run->p0 : nullptr), run->ph, c, 3, s);
+    pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 3, s);
+    c.shift = 1;   // the polar sweep is the last one: it applies the FARGO shift
+    pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, run->P.ntop, s);
+  }
   if (run->P.FARGO_flag > 0) pgk::rotate(run->T, nullptr, s);
   run->cur = 1 - a;
   run->p0_live = false;
@@ -563,15 +670,18 @@ int pg_sweep_axis(pg_run *run, int axis, double dt, const pg_body *planet, doubl
   // polar in 3D.  The dump's p is used only by a leading radial sweep.
   int n = 0;
   if (axis == 0) {
-    pgk::sweep_x(run->T, planes_fwd(run, a, run->p0_live ? run->p0 : nullptr), run->ph, c, run->P.ndim, s);
+    if (run->fp32) pgk::sweep_x32(run->T, planes32_fwd(run, a), run->ph, c, run->P.ndim, s);
+    else pgk::sweep_x(run->T, planes_fwd(run, a, run->p0_live ? run->p0 : nullptr), run->ph, c, run->P.ndim, s);
     n = nx(run);
   } else if (axis == 1) {
     c.shift = run->P.ndim == 2;
-    pgk::sweep_y(run->T, planes_fwd(run, a, nullptr), run->ph, c, run->P.ndim, s);
+    if (run->fp32) pgk::sweep_y32(run->T, planes32_fwd(run, a), run->ph, c, run->P.ndim, s);
+    else pgk::sweep_y(run->T, planes_fwd(run, a, nullptr), run->ph, c, run->P.ndim, s);
     n = ny(run);
   } else {
     c.shift = 1;
-    pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, run->P.ntop, s);
+    if (run->fp32) pgk::sweep_z32(run->T, planes32_fwd(run, a), run->ph, c, run->P.ntop, s);
+    else pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, run->P.ntop, s);
     n = nz(run);
   }
   run->cur = 1 - a;
@@ -591,8 +701,12 @@ int pg_damp(pg_run *run, double dt) {
   if (!run) return PG_ERR_ARG;
   if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
   CK(cudaSetDevice(run->dev));
-  double **cp = run->planes[run->cur];
-  pgk::damp(run->T, cp[0], cp[1], cp[2], cp[3], dt, run->P.ndim, run->stream);
+  if (run->fp32) {
+    pgk::damp32(run->T, planes32_cur(run), dt, nullptr, run->P.ndim, run->stream);
+  } else {
+    double **cp = run->planes[run->cur];
+    pgk::damp(run->T, cp[0], cp[1], cp[2], cp[3], dt, run->P.ndim, run->stream);
+  }
   return check_launch(run, 1);
 }
 
@@ -604,8 +718,12 @@ int pg_reduce(pg_run *run, const pg_body *planet, double exclude, int mode, doub
   CK(cudaSetDevice(run->dev));
   pgd::Body b{planet->m, planet->x, planet->y, planet->vx, planet->vy, planet->fx, planet->fy, planet->rs};
   exclude *= run->P.sc_h;                                 // device_func.cu:171
-  pgk::reduce(run->T, run->planes[run->cur][0], b, nullptr, exclude, mode, run->P.plnt_flag > 0,
-              run->P.p_alpha, run->P.ndim, run->ring_part, run->counter, run->dscal, nullptr, run->stream);
+  if (run->fp32)
+    pgk::reduce32(run->T, run->p32[run->cur][0], b, nullptr, exclude, mode, run->P.plnt_flag > 0,
+                  run->P.p_alpha, run->P.ndim, run->ring_part, run->counter, run->dscal, run->stream);
+  else
+    pgk::reduce(run->T, run->planes[run->cur][0], b, nullptr, exclude, mode, run->P.plnt_flag > 0,
+                run->P.p_alpha, run->P.ndim, run->ring_part, run->counter, run->dscal, nullptr, run->stream);
   if (int e = check_launch(run, 1)) return e;
   CK(cudaMemcpyAsync(out, run->dscal, sizeof(double), cudaMemcpyDeviceToHost, run->stream));
   CK(cudaStreamSynchronize(run->stream));
@@ -713,8 +831,11 @@ int pg_clock_reset(pg_run *run, int startat) {
   CK(cudaMemcpyAsync(run->clk, &c, sizeof(c), cudaMemcpyHostToDevice, s));
   // first get_dt's CFL rate (the fused loop takes later ones from sweepy)
   double **cp = run->planes[run->cur];
-  pgk::cfl_full(run->T, cp[0], cp[1], cp[2], cp[3], run->p0_live ? run->p0 : nullptr, run->ph, fr, P.ndim,
-                &run->clk->cfl_bits, s);
+  if (run->fp32)
+    pgk::cfl32(run->T, planes32_cur(run), run->ph, fr, P.ndim, 0, &run->clk->cfl_bits, nullptr, s);
+  else
+    pgk::cfl_full(run->T, cp[0], cp[1], cp[2], cp[3], run->p0_live ? run->p0 : nullptr, run->ph, fr, P.ndim,
+                  &run->clk->cfl_bits, s);
   if (int e = check_launch(run, 1)) return e;
   CK(cudaStreamSynchronize(s));
   run->clock_ready = true;
@@ -741,6 +862,47 @@ int pg_clock_get(pg_run *run, pg_clock *out, pg_body *planet) {
 }
 
 // one step of main.cu:343-441 as device work on the run's stream
+// One step of the device-resident loop on the FP32 planes: the same launch
+// sequence as the FP64 step below, with the float sweeps.
+static int enqueue_step32(pg_run *run, pgd::SweepCtl c, int n, size_t e_step) {
+  const pg_params &P = run->P;
+  cudaStream_t s = run->stream;
+  const bool tm = run->timing;
+  size_t e_k = 0;
+  int a = run->cur;
+  if (tm && ev_pair(run, 0, e_k)) return fail(run, PG_ERR_CUDA, "event record");
+  pgk::sweep_x32(run->T, planes32_fwd(run, a), run->ph, c, P.ndim, s); n += nx(run);
+  if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
+  if (P.ndim == 2) {
+    c.fuse = 1;
+    c.shift = 1;
+    if (tm && ev_pair(run, 1, e_k)) return fail(run, PG_ERR_CUDA, "event record");
+    pgk::sweep_y32(run->T, planes32_fwd(run, 1 - a), run->ph, c, 2, s); n += ny(run);
+    if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
+  } else {
+    if (tm && ev_pair(run, 1, e_k)) return fail(run, PG_ERR_CUDA, "event record");
+    pgk::sweep_y32(run->T, planes32_fwd(run, 1 - a), run->ph, c, 3, s); n += ny(run);
+    if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
+    if (tm && ev_pair(run, 2, e_k)) return fail(run, PG_ERR_CUDA, "event record");
+    c.shift = 1;
+    pgk::sweep_z32(run->T, planes32_fwd(run, a), run->ph, c, P.ntop, s); n += nz(run);
+    if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
+    run->cur = 1 - a;
+    pgk::damp32(run->T, planes32_cur(run), 0.0, run->clk, 3, s); n++;
+    pgk::cfl32_clk(run->T, planes32_cur(run), run->ph, 3, run->clk, s); n++;
+  }
+  pgk::poststep(run->clk, run->T, s); n++;
+  pgk::reduce32(run->T, run->p32[run->cur][0], pgd::Body{}, run->clk, 0.0, 0, P.plnt_flag > 0, P.p_alpha, P.ndim,
+                run->ring_part, run->counter, &run->clk->mass, s); n++;
+  if (P.plnt_flag > 0 && P.ndim == 2) {
+    pgk::reduce32(run->T, run->p32[run->cur][0], pgd::Body{}, run->clk, 0.0, 9, 1, P.p_alpha, P.ndim,
+                  run->ring_part, run->counter, &run->clk->torque, s); n++;
+  }
+  pgk::record(run->clk, s); n++;
+  if (tm && ev_close(run, e_step)) return fail(run, PG_ERR_CUDA, "event record");
+  return check_launch(run, n);
+}
+
 static int enqueue_step(pg_run *run, bool first_p0) {
   const pg_params &P = run->P;
   cudaStream_t s = run->stream;
@@ -754,6 +916,7 @@ static int enqueue_step(pg_run *run, bool first_p0) {
   size_t e_step = 0, e_k = 0;
   if (tm && ev_pair(run, 3, e_step)) return fail(run, PG_ERR_CUDA, "event record");
   pgk::prestep(run->clk, run->T, P.FARGO_flag, s); n++;
+  if (run->fp32) return enqueue_step32(run, c, n, e_step);
   if (tm && ev_pair(run, 0, e_k)) return fail(run, PG_ERR_CUDA, "event record");
   pgk::sweep_x(run->T, planes_fwd(run, a, first_p0 ? run->p0 : nullptr), run->ph, c, P.ndim, s); n += nx(run);
   if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
@@ -792,6 +955,39 @@ static int enqueue_step(pg_run *run, bool first_p0) {
   return check_launch(run, n);
 }
 
+// The device clock halts the loop (end time, a tmovie dump, an error); the
+// steps queued after that return at once.  HaltProbe bounds that waste: after
+// each launch unit (a graph replay, or a group of single steps) it queues a
+// copy of clk->halted into pinned memory, and before queueing unit i it reads
+// the copy made after unit i-kDepth, so kDepth units stay in flight.
+struct HaltProbe {
+  static constexpr int kDepth = 4;
+  pg_run *run;
+  int64_t unit = 0;
+  int init() {
+    if (run->h_halt) return PG_OK;
+    if (cudaHostAlloc(&run->h_halt, kDepth * sizeof(int), cudaHostAllocDefault) != cudaSuccess) return PG_ERR_CUDA;
+    for (auto &e : run->halt_ev)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return PG_ERR_CUDA;
+    return PG_OK;
+  }
+  // true when an earlier unit saw the clock halted
+  bool halted_before_next() {
+    if (unit < kDepth) return false;
+    int slot = (int)(unit % kDepth);
+    if (cudaEventSynchronize(run->halt_ev[slot]) != cudaSuccess) return true;   // surfaces in finish_advance
+    return run->h_halt[slot] != 0;
+  }
+  int post() {
+    int slot = (int)(unit % kDepth);
+    if (cudaMemcpyAsync(&run->h_halt[slot], &run->clk->halted, sizeof(int), cudaMemcpyDeviceToHost,
+                        run->stream) != cudaSuccess) return PG_ERR_CUDA;
+    if (cudaEventRecord(run->halt_ev[slot], run->stream) != cudaSuccess) return PG_ERR_CUDA;
+    unit++;
+    return PG_OK;
+  }
+};
+
 static int finish_advance(pg_run *run, int64_t before, int *taken) {
   pgd::DevClock c;
   CK(cudaMemcpyAsync(&c, run->clk, sizeof(c), cudaMemcpyDeviceToHost, run->stream));
@@ -817,10 +1013,15 @@ int pg_advance(pg_run *run, int nsteps, int *taken) {
   pgd::DevClock c;
   CK(cudaMemcpy(&c, run->clk, sizeof(c), cudaMemcpyDeviceToHost));
   int64_t before = c.ncycle;
+  HaltProbe hp{run};
+  if (int e = hp.init()) return fail(run, e, "halt probe set-up");
+  const int group = 16;
   for (int i = 0; i < nsteps; i++) {
+    if (i % group == 0 && hp.halted_before_next()) break;
     bool first = run->p0_live;
     if (int e = enqueue_step(run, first)) return e;
     run->p0_live = false;
+    if ((i + 1) % group == 0 && hp.post()) return fail(run, PG_ERR_CUDA, "halt probe");
   }
   return finish_advance(run, before, taken);
 }
@@ -862,13 +1063,17 @@ int pg_advance_graph(pg_run *run, int nsteps, int chunk, int *taken) {
     run->cur = cur0;
   }
   int64_t per = 0;
+  HaltProbe hp{run};
+  if (int e = hp.init()) return fail(run, e, "halt probe set-up");
   for (; done + chunk <= nsteps; done += chunk) {
+    if (hp.halted_before_next()) { done = nsteps; break; }
     size_t e = 0;
     if (run->timing && ev_pair(run, 3, e)) return fail(run, PG_ERR_CUDA, "event record");
     CK(cudaGraphLaunch(run->gexec, run->stream));
     if (run->timing && ev_close(run, e)) return fail(run, PG_ERR_CUDA, "event record");
     run->launches += run->graph_kernels;
     per++;
+    if (hp.post()) return fail(run, PG_ERR_CUDA, "halt probe");
   }
   for (; done < nsteps; done++) {
     if (int e = enqueue_step(run, false)) return e;

@@ -266,6 +266,54 @@ int pg_reduce_noalloc(const double *sigma, int64_t row_stride, const double *xc,
                       double exclude, int mode, double p_alpha, double sc_h,
                       double *out, void *stream);
 
+/* ---- batches: many disks stepped together --------------------------------
+ * No counterpart in the reference (one disk per process).  A batch steps its
+ * member runs together: per step, one launch per phase walks the pencil
+ * chunks of every 2D member of a precision group (FP64 or FP32) through a
+ * tile queue, and 3D members take their own launches in the same sequence.
+ * Each member keeps its own clock, CFL dt, end time and history, exactly as
+ * with pg_advance: a member's results do not depend on the other members or
+ * on the launch shape.  Members must be created on the batch's device,
+ * loaded and clock-reset; while in a batch they are stepped only through
+ * it.  pg_batch_advance enqueues nsteps steps of every member (members whose
+ * clock has halted idle) in CUDA graphs of `chunk` steps and returns without
+ * waiting; pg_batch_sync waits.  pg_batch_status (synchronising) reports per
+ * member, in the order added: halted (end time reached, a tmovie dump due, or
+ * an error), its status code and its step count.                           */
+typedef struct pg_batch pg_batch;
+typedef struct pg_batch_member {
+  int     halted;
+  int     status;              /* PG_OK or the run's failure code           */
+  int64_t ncycle;
+  double  simtime;
+} pg_batch_member;
+typedef struct pg_batch_shape {
+  int grid_x, grid_y;          /* CTAs of the batched radial / azimuthal
+                                  sweeps (0: one CTA per tile)              */
+  int minb;                    /* CTAs per SM the sweeps are compiled for:
+                                  8 (64 registers) or 4                     */
+  int pad;
+} pg_batch_shape;
+int pg_batch_create(int device, pg_batch **out);
+int pg_batch_destroy(pg_batch *b);
+const char *pg_batch_last_error(const pg_batch *b);
+int pg_batch_add(pg_batch *b, pg_run *run);
+int pg_batch_remove(pg_batch *b, pg_run *run);   /* synchronises */
+int pg_batch_size(const pg_batch *b);
+int pg_batch_advance(pg_batch *b, int nsteps, int chunk);
+int pg_batch_sync(pg_batch *b);
+int pg_batch_status(pg_batch *b, pg_batch_member *out, int n);
+/* launch shape per precision group (0 = FP64, 1 = FP32) */
+int pg_batch_set_shape(pg_batch *b, int group, const pg_batch_shape *shape);
+int pg_batch_get_shape(const pg_batch *b, int group, pg_batch_shape *shape);
+/* Autotuner: times `trial_steps` real steps of the members for each
+ * candidate shape of each group and keeps the fastest.  The trial steps
+ * advance the members like any others (results do not depend on the shape). */
+int pg_batch_tune(pg_batch *b, int trial_steps);
+int64_t pg_batch_launch_count(const pg_batch *b);
+/* device memory pg_create allocates for these parameters (admission) */
+size_t pg_run_device_bytes(const pg_params *p);
+
 #ifdef __cplusplus
 }
 #endif

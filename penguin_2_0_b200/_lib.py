@@ -82,6 +82,14 @@ class pg_device_view(C.Structure):
     ]
 
 
+class pg_batch_member(C.Structure):
+    _fields_ = [("halted", C.c_int), ("status", C.c_int), ("ncycle", C.c_int64), ("simtime", C.c_double)]
+
+
+class pg_batch_shape(C.Structure):
+    _fields_ = [("grid_x", C.c_int), ("grid_y", C.c_int), ("minb", C.c_int), ("pad", C.c_int)]
+
+
 _lib = None
 
 
@@ -141,6 +149,20 @@ def lib() -> C.CDLL:
         "pg_timing_read": (C.c_int, [vp, dp, C.POINTER(C.c_int64), C.c_int]),
         "pg_reduce_noalloc": (C.c_int, [vp, C.c_int64, vp, vp, vp, vp, vp, C.c_int, C.c_int, B,
                                         C.c_double, C.c_int, C.c_double, C.c_double, vp, vp]),
+        "pg_batch_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
+        "pg_batch_destroy": (C.c_int, [vp]),
+        "pg_batch_last_error": (C.c_char_p, [vp]),
+        "pg_batch_add": (C.c_int, [vp, vp]),
+        "pg_batch_remove": (C.c_int, [vp, vp]),
+        "pg_batch_size": (C.c_int, [vp]),
+        "pg_batch_advance": (C.c_int, [vp, C.c_int, C.c_int]),
+        "pg_batch_sync": (C.c_int, [vp]),
+        "pg_batch_status": (C.c_int, [vp, C.POINTER(pg_batch_member), C.c_int]),
+        "pg_batch_set_shape": (C.c_int, [vp, C.c_int, C.POINTER(pg_batch_shape)]),
+        "pg_batch_get_shape": (C.c_int, [vp, C.c_int, C.POINTER(pg_batch_shape)]),
+        "pg_batch_tune": (C.c_int, [vp, C.c_int]),
+        "pg_batch_launch_count": (C.c_int64, [vp]),
+        "pg_run_device_bytes": (C.c_size_t, [P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name, None)

@@ -72,13 +72,12 @@ __device__ __forceinline__ bool load_step(const SweepCtl &c, StepIn &s) {
 
 // ---------------------------------------------------------------------------
 // radial sweep
-template <bool SPH, bool THREED, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_sweep_x(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
-  __shared__ ChunkShmT<NT> S;
-  StepIn st;
-  if (!load_step(ctl, st)) return;
+// One radial pencil chunk: column j0, chunk l, polar layer k.  The body is
+// shared by the per-run kernel and the batched kernels of pg_batch.cu.
+template <bool SPH, bool THREED, int NT>
+__device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, const Tables &T, const Planes &P, const Phys &ph,
+                                             const SweepCtl &ctl, const StepIn &st, int j0, int l, int k) {
   const int n = threadIdx.x;
-  const int j0 = blockIdx.x, l = blockIdx.y + l0, k = blockIdx.z;
   const bool last = (l == T.cx.loop - 1);
   const int nphi = T.nphi, nrg = T.nrg;
   if (last && T.cx.stuck) {
@@ -161,16 +160,23 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_x(Tables T, Planes P, Phys p
   }
 }
 
-// ---------------------------------------------------------------------------
-// azimuthal sweep with the FARGO shift at the store and the fused epilogue
 template <bool SPH, bool THREED, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_sweep_y(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
+__global__ void __launch_bounds__(NT, MINB) k_sweep_x(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
   __shared__ ChunkShmT<NT> S;
-  __shared__ double red[NT / 32];
   StepIn st;
   if (!load_step(ctl, st)) return;
+  sweep_x_body<SPH, THREED, NT>(S, T, P, ph, ctl, st, blockIdx.x, blockIdx.y + l0, blockIdx.z);
+}
+
+// ---------------------------------------------------------------------------
+// azimuthal sweep with the FARGO shift at the store and the fused epilogue
+// One azimuthal chunk: chunk l of ring i in polar layer k; FARGO shift at
+// the store and, with ctl.fuse, damping and the CFL rate in the epilogue.
+template <bool SPH, bool THREED, int NT>
+__device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, const Tables &T, const Planes &P,
+                                             const Phys &ph, const SweepCtl &ctl, const StepIn &st, int l, int i,
+                                             int k) {
   const int n = threadIdx.x;
-  const int l = blockIdx.x + l0, i = blockIdx.y, k = blockIdx.z;
   const int nphi = T.nphi, nrg = T.nrg;
   const int row = i + NPAD;
   const int rk = k * nrg + row;
@@ -305,6 +311,15 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_y(Tables T, Planes P, Phys p
       if (anybad) atomicExch(&ctl.clk->status, 3);
     }
   }
+}
+
+template <bool SPH, bool THREED, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sweep_y(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
+  __shared__ ChunkShmT<NT> S;
+  __shared__ double red[NT / 32];
+  StepIn st;
+  if (!load_step(ctl, st)) return;
+  sweep_y_body<SPH, THREED, NT>(S, red, T, P, ph, ctl, st, blockIdx.x + l0, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -489,7 +504,7 @@ __global__ void k_cfl(Tables T, const double *R, const double *U, const double *
 }
 
 // Index_Shift orbital_advection.cu:12-43 for every interior ring
-__device__ __forceinline__ void index_shift_ring(Tables &T, int t, double dt, double FrRot, int fargo) {
+__device__ __forceinline__ void index_shift_ring(const Tables &T, int t, double dt, double FrRot, int fargo) {
   int k = t / T.nr, i = t % T.nr;
   int row = i + NPAD, rk = k * T.nrg + row;
   double xc = T.rxc[row];
@@ -608,18 +623,19 @@ __device__ __forceinline__ double tree1024(double *list) {
   return list[0];
 }
 
+// Ring i of polar layer k; the last of the run's nblocks ring blocks to
+// finish adds up the run's partial sums.
 template <typename RT>
-__global__ void __launch_bounds__(1024) k_reduce(Tables T, const RT *R, Body pl, const DevClock *clk,
-                                                 double exclude, int mode, int plnt, double p_alpha,
-                                                 int ndim, double *ring_part, unsigned int *counter,
-                                                 double *out, double *hist_row) {
+__device__ __forceinline__ void reduce_body(const Tables &T, const RT *R, Body pl, const DevClock *clk,
+                                            double exclude, int mode, int plnt, double p_alpha, int ndim,
+                                            double *ring_part, unsigned int *counter, double *out,
+                                            double *hist_row, int i, int k, unsigned nblocks) {
   __shared__ double list[1024];
   __shared__ bool is_last;
   if (clk) {
     if (!clk->prin) return;
     pl = clk->planet;
   }
-  const int i = blockIdx.x, k = blockIdx.y;
   const int row = i + NPAD, rk = k * T.nrg + row;
   const int nphi = T.nphi;
   const size_t base = (size_t)rk * nphi;
@@ -667,7 +683,7 @@ __global__ void __launch_bounds__(1024) k_reduce(Tables T, const RT *R, Body pl,
     ring_part[i + T.nr * k] = val;
     __threadfence();
     unsigned int prev = atomicAdd(counter, 1u);
-    is_last = (prev == gridDim.x * gridDim.y - 1);
+    is_last = (prev == nblocks - 1);
   }
   __syncthreads();
   if (!is_last) return;
@@ -712,8 +728,17 @@ __global__ void __launch_bounds__(1024) k_reduce(Tables T, const RT *R, Body pl,
   }
 }
 
+template <typename RT>
+__global__ void __launch_bounds__(1024) k_reduce(Tables T, const RT *R, Body pl, const DevClock *clk,
+                                                 double exclude, int mode, int plnt, double p_alpha,
+                                                 int ndim, double *ring_part, unsigned int *counter,
+                                                 double *out, double *hist_row) {
+  reduce_body<RT>(T, R, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter, out, hist_row,
+                  blockIdx.x, blockIdx.y, gridDim.x * gridDim.y);
+}
+
 // append a diagnostics row when this step prints (main.cu:414-428)
-__global__ void k_record(DevClock *clk) {
+__device__ __forceinline__ void record_body(DevClock *clk) {
   DevClock &c = *clk;
   if (!c.prin) return;
   if (c.hist && c.hist_count < c.hist_cap) {
@@ -732,6 +757,8 @@ __global__ void k_record(DevClock *clk) {
   }
   c.prin = 0;
 }
+
+__global__ void k_record(DevClock *clk) { record_body(clk); }
 
 // ---------------------------------------------------------------------------
 // planet (planet.cu:28-93), device copies of the host arithmetic
@@ -762,7 +789,7 @@ __device__ void d_forces_fixed(Body &pl, double FrRot) {
 }
 
 // get_dt host part + dt clipping + Index_Shift + half kick (main.cu:345-370)
-__global__ void k_prestep(DevClock *clk, Tables T, int fargo) {
+__device__ __forceinline__ void prestep_body(DevClock *clk, const Tables &T, int fargo) {
   __shared__ double s_dt, s_frrot;
   __shared__ int s_run;
   if (threadIdx.x == 0) {
@@ -808,8 +835,10 @@ __global__ void k_prestep(DevClock *clk, Tables T, int fargo) {
   for (int t = threadIdx.x; t < T.nr * T.nk; t += blockDim.x) index_shift_ring(T, t, s_dt, s_frrot, fargo);
 }
 
+__global__ void k_prestep(DevClock *clk, Tables T, int fargo) { prestep_body(clk, T, fargo); }
+
 // simtime/drift/forces/kick/dump bookkeeping (main.cu:378-412)
-__global__ void k_poststep(DevClock *clk, Tables T) {
+__device__ __forceinline__ void poststep_body(DevClock *clk, const Tables &T) {
   int t = threadIdx.x;
   DevClock &c = *clk;
   int halted = c.halted;
@@ -841,6 +870,85 @@ __global__ void k_poststep(DevClock *clk, Tables T) {
     c.halted = 1;   // the host dumps before continuing
   }
   if (c.done) c.halted = 1;
+}
+
+__global__ void k_poststep(DevClock *clk, Tables T) { poststep_body(clk, T); }
+
+// ---------------------------------------------------------------------------
+// Batched 2D steps: one launch per phase walks the tiles of every run of a
+// group.  A tile is one pencil chunk (sweeps) or one ring (reductions); the
+// run of tile t is found by bisection in the queue's prefix sums.  Each
+// tile runs the same body as the per-run kernels, so a run's results do not
+// depend on the batch it is in or on the launch shape.
+__device__ __forceinline__ int batch_find(const BatchQueue &q, int t) {
+  int lo = 0, hi = q.nruns;   // q.start[lo] <= t < q.start[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (q.start[mid] <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void kb_prestep(const BatchRun *runs) {
+  const BatchRun &b = runs[blockIdx.x];
+  prestep_body(b.clk, b.T, b.fargo);
+}
+__global__ void kb_poststep(const BatchRun *runs) {
+  const BatchRun &b = runs[blockIdx.x];
+  poststep_body(b.clk, b.T);
+}
+__global__ void kb_record(const BatchRun *runs) { record_body(runs[blockIdx.x].clk); }
+
+template <typename RT>
+__global__ void __launch_bounds__(1024) kb_reduce(BatchQueue q, int mode) {
+  const int r = batch_find(q, blockIdx.x);
+  const BatchRun &b = q.runs[r];
+  if (mode == 9 && !b.plnt) return;
+  const RT *R;
+  if constexpr (sizeof(RT) == 4) R = (const RT *)b.QX.r;   // a 2D step ends in its first planes
+  else R = (const RT *)b.PX.r;
+  double *out = (mode == 0) ? &b.clk->mass : &b.clk->torque;
+  reduce_body<RT>(b.T, R, Body{}, b.clk, 0.0, mode, mode == 9 ? 1 : b.plnt, b.p_alpha, 2, b.ring_part, b.counter,
+                  out, nullptr, blockIdx.x - q.start[r], 0, (unsigned)b.T.nr);
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) kb_sweep_x(BatchQueue q) {
+  __shared__ ChunkShmT<128> S;
+  for (int t = blockIdx.x; t < q.total; t += gridDim.x) {
+    const int r = batch_find(q, t);
+    const BatchRun &b = q.runs[r];
+    SweepCtl ctl{};
+    ctl.clk = b.clk;
+    StepIn st;
+    if (load_step(ctl, st)) {
+      const int lt = t - q.start[r], nphi = b.T.nphi;
+      Planes P = b.PX;
+      P.p0 = (b.p0 && b.clk->ncycle == b.p0_cycle) ? b.p0 : nullptr;
+      sweep_x_body<false, false, 128>(S, b.T, P, b.ph, ctl, st, lt % nphi, lt / nphi, 0);
+    }
+    __syncthreads();
+  }
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) kb_sweep_y(BatchQueue q) {
+  __shared__ ChunkShmT<128> S;
+  __shared__ double red[4];
+  for (int t = blockIdx.x; t < q.total; t += gridDim.x) {
+    const int r = batch_find(q, t);
+    const BatchRun &b = q.runs[r];
+    SweepCtl ctl{};
+    ctl.clk = b.clk;
+    ctl.fuse = 1;
+    ctl.shift = 1;
+    StepIn st;
+    if (load_step(ctl, st)) {
+      const int lt = t - q.start[r], loop = b.T.cy.loop;
+      sweep_y_body<false, false, 128>(S, red, b.T, b.PY, b.ph, ctl, st, lt % loop, lt / loop, 0);
+    }
+    __syncthreads();
+  }
 }
 
 }  // namespace pgd
@@ -994,6 +1102,34 @@ void tables(const Tables &T, const Phys &ph, int ndim, double kill_rin, double k
             double xmax, cudaStream_t s) {
   int n = T.nk * T.nrg;
   k_tables<<<(n + 127) / 128, 128, 0, s>>>(T, ph, ndim, kill_rin, kill_rout, xmin, xmax);
+}
+
+
+void batch_prestep(const BatchRun *runs, int nruns, cudaStream_t s) {
+  if (nruns > 0) kb_prestep<<<nruns, 256, 0, s>>>(runs);
+}
+void batch_poststep(const BatchRun *runs, int nruns, cudaStream_t s) {
+  if (nruns > 0) kb_poststep<<<nruns, 256, 0, s>>>(runs);
+}
+void batch_record(const BatchRun *runs, int nruns, cudaStream_t s) {
+  if (nruns > 0) kb_record<<<nruns, 1, 0, s>>>(runs);
+}
+void batch_reduce(const BatchQueue &rings, int fp32, int mode, cudaStream_t s) {
+  if (rings.total <= 0) return;
+  if (fp32) kb_reduce<float><<<rings.total, 1024, 0, s>>>(rings, mode);
+  else kb_reduce<double><<<rings.total, 1024, 0, s>>>(rings, mode);
+}
+void batch_sweep_x(const BatchQueue &q, int grid, int minb, cudaStream_t s) {
+  if (q.total <= 0) return;
+  int g = (grid > 0 && grid < q.total) ? grid : q.total;
+  if (minb >= 8) kb_sweep_x<8><<<g, 128, 0, s>>>(q);
+  else kb_sweep_x<4><<<g, 128, 0, s>>>(q);
+}
+void batch_sweep_y(const BatchQueue &q, int grid, int minb, cudaStream_t s) {
+  if (q.total <= 0) return;
+  int g = (grid > 0 && grid < q.total) ? grid : q.total;
+  if (minb >= 8) kb_sweep_y<8><<<g, 128, 0, s>>>(q);
+  else kb_sweep_y<4><<<g, 128, 0, s>>>(q);
 }
 
 }  // namespace pgk

@@ -81,6 +81,30 @@ struct SweepCtl {
   int shift;          // store at (j + inc_j) mod jmax: the last sweep of a step
 };
 
+// One run of a batch (pg_batch.cu): what its kernels read, in device memory.
+struct BatchRun {
+  Tables T;
+  Phys ph;
+  DevClock *clk;
+  Planes PX, PY;          // FP64 runs: planes of the radial and of the azimuthal sweep
+  Planes32 QX, QY;        // FP32 runs
+  const double *p0;       // FP64 run with a freshly loaded dump: its pressure plane,
+  long long p0_cycle;     //   read by the radial sweep of the step with ncycle == p0_cycle
+  double *ring_part;
+  unsigned int *counter;
+  double p_alpha;
+  int fargo, plnt;
+};
+
+// A group of runs walked by one launch: tile t belongs to run r when
+// start[r] <= t < start[r + 1].
+struct BatchQueue {
+  const BatchRun *runs;
+  const int *start;       // [nruns + 1] device prefix sums
+  int nruns;
+  int total;
+};
+
 }  // namespace pgd
 
 // launchers (pg_kernels.cu)
@@ -112,6 +136,15 @@ void cfl32(const Tables &T, const Planes32 &cur, const Phys &ph, double frrot, i
            unsigned long long *out, int *status, cudaStream_t s);
 void damp32(const Tables &T, const Planes32 &cur, double dt, const DevClock *clk, int ndim, cudaStream_t s);
 void cfl32_clk(const Tables &T, const Planes32 &cur, const Phys &ph, int ndim, DevClock *clk, cudaStream_t s);
+// batched 2D steps over many runs (one launch per phase for all runs)
+void batch_prestep(const BatchRun *runs, int nruns, cudaStream_t s);
+void batch_poststep(const BatchRun *runs, int nruns, cudaStream_t s);
+void batch_record(const BatchRun *runs, int nruns, cudaStream_t s);
+void batch_reduce(const BatchQueue &rings, int fp32, int mode, cudaStream_t s);
+void batch_sweep_x(const BatchQueue &q, int grid, int minb, cudaStream_t s);
+void batch_sweep_y(const BatchQueue &q, int grid, int minb, cudaStream_t s);
+void batch_sweep_x32(const BatchQueue &q, int grid, int minb, cudaStream_t s);
+void batch_sweep_y32(const BatchQueue &q, int grid, int minb, cudaStream_t s);
 void damp_clk(const Tables &T, double *r, double *u, double *v, double *w, const DevClock *clk,
               cudaStream_t s);
 void cfl_clk(const Tables &T, const double *r, const double *u, const double *v, const double *w,

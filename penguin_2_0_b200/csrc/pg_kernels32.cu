@@ -69,13 +69,13 @@ __device__ __forceinline__ void derivs_w(T &first, T &second, int n, const float
 }
 
 // ---------------------------------------------------------------------------
-template <bool SPH, bool THREED, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k32_sweep_x(Tables T, Planes32 P, Phys ph, SweepCtl ctl, int l0) {
-  __shared__ ChunkShm32<NT> S;
-  StepIn32 st;
-  if (!load_step32(ctl, st)) return;
+// One radial pencil chunk: column j0, chunk l, polar layer k.  The body is
+// shared by the per-run kernel and the batched kernels of pg_batch.cu.
+template <bool SPH, bool THREED, int NT>
+__device__ __forceinline__ void sweep_x32_body(ChunkShm32<NT> &S, const Tables &T, const Planes32 &P,
+                                               const Phys &ph, const SweepCtl &ctl, const StepIn32 &st,
+                                               int j0, int l, int k) {
   const int n = threadIdx.x;
-  const int j0 = blockIdx.x, l = blockIdx.y + l0, k = blockIdx.z;
   const bool last = (l == T.cx.loop - 1);
   const int nphi = T.nphi, nrg = T.nrg;
   if (last && T.cx.stuck) {
@@ -163,15 +163,22 @@ __global__ void __launch_bounds__(NT, MINB) k32_sweep_x(Tables T, Planes32 P, Ph
   }
 }
 
-// ---------------------------------------------------------------------------
 template <bool SPH, bool THREED, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k32_sweep_y(Tables T, Planes32 P, Phys ph, SweepCtl ctl, int l0) {
+__global__ void __launch_bounds__(NT, MINB) k32_sweep_x(Tables T, Planes32 P, Phys ph, SweepCtl ctl, int l0) {
   __shared__ ChunkShm32<NT> S;
-  __shared__ double red[NT / 32];
   StepIn32 st;
   if (!load_step32(ctl, st)) return;
+  sweep_x32_body<SPH, THREED, NT>(S, T, P, ph, ctl, st, blockIdx.x, blockIdx.y + l0, blockIdx.z);
+}
+
+// ---------------------------------------------------------------------------
+// One azimuthal chunk: chunk l of ring i in polar layer k; FARGO shift at
+// the store and, with ctl.fuse, damping and the CFL rate in the epilogue.
+template <bool SPH, bool THREED, int NT>
+__device__ __forceinline__ void sweep_y32_body(ChunkShm32<NT> &S, double *red, const Tables &T,
+                                               const Planes32 &P, const Phys &ph, const SweepCtl &ctl,
+                                               const StepIn32 &st, int l, int i, int k) {
   const int n = threadIdx.x;
-  const int l = blockIdx.x + l0, i = blockIdx.y, k = blockIdx.z;
   const int nphi = T.nphi, nrg = T.nrg;
   const int row = i + NPAD;
   const int rk = k * nrg + row;
@@ -307,6 +314,15 @@ __global__ void __launch_bounds__(NT, MINB) k32_sweep_y(Tables T, Planes32 P, Ph
       if (anybad) atomicExch(&ctl.clk->status, 3);
     }
   }
+}
+
+template <bool SPH, bool THREED, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k32_sweep_y(Tables T, Planes32 P, Phys ph, SweepCtl ctl, int l0) {
+  __shared__ ChunkShm32<NT> S;
+  __shared__ double red[NT / 32];
+  StepIn32 st;
+  if (!load_step32(ctl, st)) return;
+  sweep_y32_body<SPH, THREED, NT>(S, red, T, P, ph, ctl, st, blockIdx.x + l0, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -491,6 +507,55 @@ __global__ void k32_damp(Tables T, float *R, float *U, float *V, float *W, doubl
   }
 }
 
+// ---------------------------------------------------------------------------
+// Batched FP32 sweeps: tiles of every run of a group in one launch (see the
+// FP64 batched kernels in pg_kernels.cu for the tile queue).
+__device__ __forceinline__ int batch_find32(const BatchQueue &q, int t) {
+  int lo = 0, hi = q.nruns;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (q.start[mid] <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) kb32_sweep_x(BatchQueue q) {
+  __shared__ ChunkShm32<128> S;
+  for (int t = blockIdx.x; t < q.total; t += gridDim.x) {
+    const int r = batch_find32(q, t);
+    const BatchRun &b = q.runs[r];
+    SweepCtl ctl{};
+    ctl.clk = b.clk;
+    StepIn32 st;
+    if (load_step32(ctl, st)) {
+      const int lt = t - q.start[r], nphi = b.T.nphi;
+      sweep_x32_body<false, false, 128>(S, b.T, b.QX, b.ph, ctl, st, lt % nphi, lt / nphi, 0);
+    }
+    __syncthreads();
+  }
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) kb32_sweep_y(BatchQueue q) {
+  __shared__ ChunkShm32<128> S;
+  __shared__ double red[4];
+  for (int t = blockIdx.x; t < q.total; t += gridDim.x) {
+    const int r = batch_find32(q, t);
+    const BatchRun &b = q.runs[r];
+    SweepCtl ctl{};
+    ctl.clk = b.clk;
+    ctl.fuse = 1;
+    ctl.shift = 1;
+    StepIn32 st;
+    if (load_step32(ctl, st)) {
+      const int lt = t - q.start[r], loop = b.T.cy.loop;
+      sweep_y32_body<false, false, 128>(S, red, b.T, b.QY, b.ph, ctl, st, lt % loop, lt / loop, 0);
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace pgd
 
 namespace pgk {
@@ -573,6 +638,20 @@ void cfl32_clk(const Tables &T, const Planes32 &cur, const Phys &ph, int ndim, D
 void damp32(const Tables &T, const Planes32 &cur, double dt, const DevClock *clk, int ndim, cudaStream_t s) {
   dim3 grid(T.nr, T.nk);
   k32_damp<<<grid, 256, 0, s>>>(T, cur.ro, cur.uo, cur.vo, cur.wo, dt, clk, ndim);
+}
+
+
+void batch_sweep_x32(const BatchQueue &q, int grid, int minb, cudaStream_t s) {
+  if (q.total <= 0) return;
+  int g = (grid > 0 && grid < q.total) ? grid : q.total;
+  if (minb >= 8) kb32_sweep_x<8><<<g, 128, 0, s>>>(q);
+  else kb32_sweep_x<4><<<g, 128, 0, s>>>(q);
+}
+void batch_sweep_y32(const BatchQueue &q, int grid, int minb, cudaStream_t s) {
+  if (q.total <= 0) return;
+  int g = (grid > 0 && grid < q.total) ? grid : q.total;
+  if (minb >= 8) kb32_sweep_y<8><<<g, 128, 0, s>>>(q);
+  else kb32_sweep_y<4><<<g, 128, 0, s>>>(q);
 }
 
 }  // namespace pgk

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "pg_host.h"
+#include "pg_internal.h"
 #include "pg_kernels.cuh"
 
 using pgd::NPAD;
@@ -65,6 +66,7 @@ struct pg_run {
   // captured step graphs
   cudaGraphExec_t gexec = nullptr;
   int gsteps = 0;
+  int gcur = 0;                    // plane copy current when gexec was captured
   int64_t graph_kernels = 0;       // kernels per replay of gexec
   // early exit of pg_advance*: pinned copies of clk->halted, read a few
   // launches behind the one being queued
@@ -1041,9 +1043,10 @@ int pg_advance_graph(pg_run *run, int nsteps, int chunk, int *taken) {
     run->p0_live = false;
     done = 1;
   }
-  if (!run->gexec || run->gsteps != chunk) {
+  if (!run->gexec || run->gsteps != chunk || run->gcur != run->cur) {
     if (run->gexec) { cudaGraphExecDestroy(run->gexec); run->gexec = nullptr; }
     int cur0 = run->cur;
+    run->gcur = cur0;   // 3D steps flip the plane copies: the graph is valid for this one
     bool tm = run->timing;
     run->timing = false;
     int64_t l0 = run->launches;
@@ -1122,3 +1125,89 @@ int pg_history(pg_run *run, double *rows, int max, int *rows_out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// device footprint of a run (pg_create's allocations), for admission control
+extern "C" size_t pg_run_device_bytes(const pg_params *p) {
+  if (!p) return 0;
+  auto up = [](size_t b) { return (b + 511) & ~(size_t)511; };
+  size_t nr = (size_t)p->imax, nphi = (size_t)p->jmax, nk = (size_t)p->kmax, nrg = nr + 2 * NPAD;
+  size_t nring = nk * nrg, nz = nk + 2 * NPAD;
+  size_t pe = nring * nphi;
+  int nf = (p->ndim == 3) ? 4 : 3;
+  size_t es = (p->precision == 1) ? sizeof(float) : sizeof(double);
+  size_t b = 2 * (size_t)nf * up(pe * es);
+  if (p->precision != 1) b += up(pe * sizeof(double));                         // p0
+  b += up((4 * nrg + 10 * nring + 4 * nphi + 4 * nz + 2 * NPAD * nr * 4) * sizeof(double));
+  b += up(2 * nring * sizeof(int)) + 3 * up(nring * sizeof(double));           // itab, rot_v, vbg, sbg
+  b += up(nr * nk * sizeof(double)) + up(4) + up(32) + up(8) + up(sizeof(pgd::DevClock));
+  b += up((size_t)4096 * pgd::HIST_COLS * sizeof(double));
+  return b;
+}
+
+namespace pgi {
+
+int run_shape(const pg_run *run, RunShape *o) {
+  if (!run || !o) return PG_ERR_ARG;
+  o->dev = run->dev;
+  o->ndim = run->P.ndim;
+  o->fp32 = run->fp32 ? 1 : 0;
+  o->loaded = run->loaded ? 1 : 0;
+  o->clock_ready = run->clock_ready ? 1 : 0;
+  o->p0_live = run->p0_live ? 1 : 0;
+  o->nr = run->nr; o->nphi = run->nphi; o->nk = run->nk;
+  o->tiles_x = run->nphi * run->T.cx.loop * run->nk;
+  o->tiles_y = run->T.cy.loop * run->nr * run->nk;
+  return PG_OK;
+}
+
+int run_batch_desc(pg_run *run, pgd::BatchRun *d) {
+  if (!run || !d) return PG_ERR_ARG;
+  if (!run->clock_ready) return fail(run, PG_ERR_STATE, "batch member needs pg_clock_reset first");
+  std::memset((void *)d, 0, sizeof(*d));
+  d->T = run->T;
+  d->ph = run->ph;
+  d->clk = run->clk;
+  int a = run->cur;
+  if (run->fp32) {
+    d->QX = planes32_fwd(run, a);
+    d->QY = planes32_fwd(run, 1 - a);
+  } else {
+    d->PX = planes_fwd(run, a, nullptr);
+    d->PY = planes_fwd(run, 1 - a, nullptr);
+    if (run->p0_live) {
+      pgd::DevClock c;
+      CK(cudaMemcpy(&c, run->clk, sizeof(c), cudaMemcpyDeviceToHost));
+      d->p0 = run->p0;
+      d->p0_cycle = c.ncycle;
+    }
+  }
+  d->ring_part = run->ring_part;
+  d->counter = run->counter;
+  d->p_alpha = run->P.p_alpha;
+  d->fargo = run->P.FARGO_flag;
+  d->plnt = run->P.plnt_flag > 0;
+  return PG_OK;
+}
+
+void run_batched(pg_run *run, int64_t launches) {
+  run->p0_live = false;
+  run->launches += launches;
+}
+
+int run_enqueue_on(pg_run *run, cudaStream_t s, int64_t *launches) {
+  cudaStream_t own = run->stream;
+  int64_t l0 = run->launches;
+  run->stream = s;
+  int st = enqueue_step(run, run->p0_live);
+  run->stream = own;
+  run->p0_live = false;
+  if (launches) *launches += run->launches - l0;
+  return st;
+}
+
+pgd::DevClock *run_clock(pg_run *run) { return run->clk; }
+int run_cur(const pg_run *run) { return run->cur; }
+cudaStream_t run_stream(pg_run *run) { return run->stream; }
+
+}  // namespace pgi

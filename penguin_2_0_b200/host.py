@@ -288,6 +288,83 @@ class Run:
         return s, simtime, dt, planet, FrRot
 
 
+class Batch:
+    """Many runs stepped together (include/penguin_b200.h, pg_batch_*).
+
+    Members are Run objects that are loaded and clock-reset; each keeps its own
+    clock and dt.  While a run is in a batch, step it only through the batch."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(_lib.lib().pg_batch_create(device, C.byref(h)), None, "pg_batch_create")
+        self._h = h
+        self.members: list[Run] = []
+
+    def _ck(self, st: int, what: str):
+        if st != 0:
+            msg = _lib.lib().pg_batch_last_error(self._h) or b""
+            raise PenguinError(st, f"{what}: {msg.decode(errors='replace')}")
+
+    def close(self):
+        if self._h:
+            _lib.lib().pg_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, run: Run) -> "Batch":
+        self._ck(_lib.lib().pg_batch_add(self._h, run._h), "pg_batch_add")
+        self.members.append(run)
+        return self
+
+    def remove(self, run: Run):
+        self._ck(_lib.lib().pg_batch_remove(self._h, run._h), "pg_batch_remove")
+        self.members.remove(run)
+
+    def advance(self, nsteps: int, chunk: int = 32):
+        self._ck(_lib.lib().pg_batch_advance(self._h, nsteps, chunk), "pg_batch_advance")
+
+    def sync(self):
+        self._ck(_lib.lib().pg_batch_sync(self._h), "pg_batch_sync")
+
+    def status(self) -> list[dict]:
+        n = len(self.members)
+        arr = (_lib.pg_batch_member * max(n, 1))()
+        self._ck(_lib.lib().pg_batch_status(self._h, arr, n), "pg_batch_status")
+        return [dict(halted=arr[i].halted, status=arr[i].status, ncycle=arr[i].ncycle,
+                     simtime=arr[i].simtime) for i in range(n)]
+
+    def shape(self, group: int) -> dict:
+        sh = _lib.pg_batch_shape()
+        self._ck(_lib.lib().pg_batch_get_shape(self._h, group, C.byref(sh)), "pg_batch_get_shape")
+        return dict(grid_x=sh.grid_x, grid_y=sh.grid_y, minb=sh.minb)
+
+    def set_shape(self, group: int, grid_x: int = 0, grid_y: int = 0, minb: int = 8):
+        sh = _lib.pg_batch_shape(grid_x, grid_y, minb, 0)
+        self._ck(_lib.lib().pg_batch_set_shape(self._h, group, C.byref(sh)), "pg_batch_set_shape")
+
+    def tune(self, trial_steps: int = 8):
+        self._ck(_lib.lib().pg_batch_tune(self._h, trial_steps), "pg_batch_tune")
+
+    def launches(self) -> int:
+        return int(_lib.lib().pg_batch_launch_count(self._h))
+
+
+def run_device_bytes(p: pg_params) -> int:
+    """Device memory pg_create allocates for these parameters."""
+    return int(_lib.lib().pg_run_device_bytes(C.byref(p)))
+
+
 # ---- the reference's free functions ----------------------------------------------
 def get_dt(dt: float, run: Run, FrRot: float = 0.0) -> float:
     out = C.c_double(0.0)

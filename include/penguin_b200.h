@@ -311,8 +311,41 @@ int pg_batch_get_shape(const pg_batch *b, int group, pg_batch_shape *shape);
  * advance the members like any others (results do not depend on the shape). */
 int pg_batch_tune(pg_batch *b, int trial_steps);
 int64_t pg_batch_launch_count(const pg_batch *b);
+/* the cudaStream_t the batch launches on (for events around its work) */
+void *pg_batch_stream(const pg_batch *b);
 /* device memory pg_create allocates for these parameters (admission) */
 size_t pg_run_device_bytes(const pg_params *p);
+
+/* ---- serving: continuous batching of arriving disk runs -------------------
+ * A server steps every admitted run in one pg_batch.  pg_server_run_trace
+ * replays an arrival trace (requests sorted by arrival time, seconds from the
+ * call) against the wall clock: requests queue in arrival order; the head is
+ * admitted when fewer than max_slots runs are live and its footprint
+ * (pg_run_device_bytes) fits in what is left of hbm_budget; each round
+ * enqueues `chunk` steps of all live runs, admits arrivals while they run,
+ * then retires runs whose clock halted at their end time.  out[i] receives
+ * request i's times (arrival, admission, completion), steps and status.
+ * With keep_results, each finished run's final dump stays on the host until
+ * pg_server_result copies it out (same layout as pg_save_rings).          */
+typedef struct pg_server pg_server;
+typedef struct pg_completion {
+  int64_t id;
+  double  arrival_s, admit_s, finish_s;   /* seconds from the start of the trace */
+  int64_t steps;
+  int64_t cells;
+  double  simtime;
+  int     status;                         /* PG_OK, or the run's failure code */
+  int     pad;
+} pg_completion;
+int pg_server_create(int device, size_t hbm_budget, int max_slots, int chunk, int keep_results,
+                     pg_server **out);
+int pg_server_destroy(pg_server *s);
+const char *pg_server_last_error(const pg_server *s);
+int pg_server_run_trace(pg_server *s, const pg_params *reqs, const double *arrival_s, const int64_t *ids,
+                        int n, pg_completion *out);
+int pg_server_result(pg_server *s, int64_t id, void *rings, size_t bytes);
+int64_t pg_server_rounds(const pg_server *s);
+int pg_server_batch(pg_server *s, pg_batch **out);
 
 #ifdef __cplusplus
 }

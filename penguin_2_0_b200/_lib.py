@@ -90,6 +90,12 @@ class pg_batch_shape(C.Structure):
     _fields_ = [("grid_x", C.c_int), ("grid_y", C.c_int), ("minb", C.c_int), ("pad", C.c_int)]
 
 
+class pg_completion(C.Structure):
+    _fields_ = [("id", C.c_int64), ("arrival_s", C.c_double), ("admit_s", C.c_double), ("finish_s", C.c_double),
+                ("steps", C.c_int64), ("cells", C.c_int64), ("simtime", C.c_double), ("status", C.c_int),
+                ("pad", C.c_int)]
+
+
 _lib = None
 
 
@@ -162,7 +168,15 @@ def lib() -> C.CDLL:
         "pg_batch_get_shape": (C.c_int, [vp, C.c_int, C.POINTER(pg_batch_shape)]),
         "pg_batch_tune": (C.c_int, [vp, C.c_int]),
         "pg_batch_launch_count": (C.c_int64, [vp]),
+        "pg_batch_stream": (vp, [vp]),
         "pg_run_device_bytes": (C.c_size_t, [P]),
+        "pg_server_create": (C.c_int, [C.c_int, C.c_size_t, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
+        "pg_server_destroy": (C.c_int, [vp]),
+        "pg_server_last_error": (C.c_char_p, [vp]),
+        "pg_server_run_trace": (C.c_int, [vp, P, dp, C.POINTER(C.c_int64), C.c_int, C.POINTER(pg_completion)]),
+        "pg_server_result": (C.c_int, [vp, C.c_int64, vp, C.c_size_t]),
+        "pg_server_rounds": (C.c_int64, [vp]),
+        "pg_server_batch": (C.c_int, [vp, C.POINTER(vp)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name, None)

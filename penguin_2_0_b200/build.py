@@ -13,7 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libpenguin_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]
-SOURCES = ["pg_host.cpp", "pg_kernels.cu", "pg_kernels32.cu", "pg_run.cu", "pg_batch.cu", "pg_noalloc.cu"]
+SOURCES = ["pg_host.cpp", "pg_kernels.cu", "pg_kernels32.cu", "pg_run.cu", "pg_batch.cu", "pg_serve.cpp", "pg_noalloc.cu"]
 
 
 def _newer(out, deps):

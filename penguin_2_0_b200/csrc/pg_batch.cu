@@ -93,6 +93,7 @@ static void drop_graph(pg_batch *b) {
 
 // descriptors, tile prefix sums and the status arrays for the current members
 static int rebuild(pg_batch *b) {
+  BK(cudaStreamSynchronize(b->stream));   // in-flight steps read the old descriptors
   drop_graph(b);
   for (auto &g : b->g) g.members.clear();
   b->solo.clear();
@@ -429,5 +430,7 @@ int pg_batch_tune(pg_batch *b, int trial_steps) {
 }
 
 int64_t pg_batch_launch_count(const pg_batch *b) { return b ? b->launches : 0; }
+
+void *pg_batch_stream(const pg_batch *b) { return b ? (void *)b->stream : nullptr; }
 
 }  // extern "C"

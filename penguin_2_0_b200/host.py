@@ -359,6 +359,62 @@ class Batch:
     def launches(self) -> int:
         return int(_lib.lib().pg_batch_launch_count(self._h))
 
+    def stream_ptr(self) -> int:
+        return _lib.lib().pg_batch_stream(self._h) or 0
+
+
+class Server:
+    """Continuous-batching serving loop (include/penguin_b200.h, pg_server_*)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 150 * 10 ** 9, max_slots: int = 64,
+                 chunk: int = 32, keep_results: bool = False):
+        h = C.c_void_p()
+        _check(_lib.lib().pg_server_create(device, hbm_budget, max_slots, chunk, 1 if keep_results else 0,
+                                           C.byref(h)), None, "pg_server_create")
+        self._h = h
+
+    def _ck(self, st: int, what: str):
+        if st != 0:
+            msg = _lib.lib().pg_server_last_error(self._h) or b""
+            raise PenguinError(st, f"{what}: {msg.decode(errors='replace')}")
+
+    def close(self):
+        if self._h:
+            _lib.lib().pg_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run_trace(self, reqs: list, arrival_s, ids=None) -> list[dict]:
+        n = len(reqs)
+        arr = (pg_params * max(n, 1))(*reqs)
+        t = (C.c_double * max(n, 1))(*[float(x) for x in arrival_s])
+        ids = list(range(n)) if ids is None else list(ids)
+        ii = (C.c_int64 * max(n, 1))(*ids)
+        out = (_lib.pg_completion * max(n, 1))()
+        self._ck(_lib.lib().pg_server_run_trace(self._h, arr, t, ii, n, out), "pg_server_run_trace")
+        keys = [f for f, _ in _lib.pg_completion._fields_ if f != "pad"]
+        return [{k: getattr(out[i], k) for k in keys} for i in range(n)]
+
+    def result(self, rid: int, p: pg_params) -> bytearray:
+        buf = bytearray(ring_bytes(p.jmax) * p.imax * p.kmax)
+        c = (C.c_char * len(buf)).from_buffer(buf)
+        self._ck(_lib.lib().pg_server_result(self._h, rid, c, len(buf)), "pg_server_result")
+        return buf
+
+    def rounds(self) -> int:
+        return int(_lib.lib().pg_server_rounds(self._h))
+
 
 def run_device_bytes(p: pg_params) -> int:
     """Device memory pg_create allocates for these parameters."""

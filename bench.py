@@ -55,6 +55,8 @@ WORKLOADS = {
     "big": (0, {"imax": 4096, "jmax": 12288}, "2D r-phi disk 4096x12288 FP64, same disk"),
     "prof": (0, {"imax": 2048, "jmax": 6144}, "2D r-phi disk 2048x6144 FP64 (profiling case, > L2)"),
     "prof32": (0, {"imax": 2048, "jmax": 6144, "precision": 1}, "2D r-phi disk 2048x6144 FP32 planes (> L2)"),
+    "ens": (None, {}, "batched ensemble of 64 2D disks (configs[3])"),
+    "serve": (None, {}, "serving stream (configs[4] sample)"),
 }
 
 
@@ -168,7 +170,14 @@ def run_reference(args):
     import penguin_2_0_b200 as pg
     from oracle.pyoracle import Oracle
     which, over, desc = WORKLOADS[args.workload]
-    p = pg.params(which, **over)
+    if which is None:
+        # batched workloads: the CPU restatement advances their first disk
+        from penguin_2_0_b200 import ensemble as E
+        p = E.draw_ensemble(1, seed=0)[0]
+        p.precision = 0
+        desc = f"{desc}: its first disk ({p.imax}x{p.jmax}) on the CPU"
+    else:
+        p = pg.params(which, **over)
     p.nprin = 1
     cells = p.imax * p.jmax * p.kmax
     orc = Oracle(p, pg.build_ic(p))
@@ -200,6 +209,143 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def _plain_cfg0(pg, torch, steps: int = 100) -> float:
+    """The plain FP64 path on the 256x768 disk (one disk, L2 flushed between
+    steps, CUDA events): the reference point of the batched ensemble."""
+    p = pg.params(0, nprin=100, endtime=1e9, tmovie=1e9)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    with pg.Run(p, torch.cuda.current_device()) as run:
+        run.load(pg.build_ic(p))
+        run.clock_reset(0)
+        run.advance(5, graph_chunk=1)
+        run.timing(True)
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            run.advance(1, graph_chunk=1)
+        ms, _ = run.timing_read()
+    return p.imax * p.jmax * steps / (ms[3] / 1e3)
+
+
+def bench_ensemble(args):
+    """Batched ensemble: 64 seeded 2D disks (nr in {128..512}, nphi = 3 nr,
+    q, h, alpha, slope drawn per disk) advanced 10 orbits each in one batch;
+    FP32 planes where the thermal-mass policy allows, FP64 elsewhere."""
+    import torch
+    import penguin_2_0_b200 as pg
+    from penguin_2_0_b200 import ensemble as E
+    torch.cuda.set_device(0)
+    n = int(os.environ.get("PG_ENS_N", "64"))
+    orbits = float(os.environ.get("PG_ENS_ORBITS", "10"))
+    ps = E.draw_ensemble(n, seed=0, orbits=orbits)
+    n32 = sum(p.precision for p in ps)
+    ics = [pg.build_ic(p) for p in ps]
+    ev, clocks = {}, ClockSampler(0)
+
+    def on_start(b):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(torch.cuda.ExternalStream(b.stream_ptr()))
+        ev["a"] = e
+        clocks.start()
+
+    def on_stop(b):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(torch.cuda.ExternalStream(b.stream_ptr()))
+        e.synchronize()
+        ev["b"] = e
+
+    t0 = time.perf_counter()
+    res = E.run_ensemble(ps, ics=ics, chunk=args.chunk, tune_steps=2, keep_dumps=True,
+                         on_start=on_start, on_stop=on_stop)
+    e2e_el = time.perf_counter() - t0
+    clk = clocks.stop()
+    dev_s = ev["a"].elapsed_time(ev["b"]) / 1e3
+    value = res.cell_updates / dev_s
+    all_updates = sum(E.disk_cells(p) * s for p, s in zip(ps, res.steps))
+    dump_bytes = sum(len(ic) for ic in ics)
+    max_steps = max(res.steps)
+    plain = _plain_cfg0(pg, torch)
+    cpu = None
+    if not args.no_cpu:
+        v, done, cores, el = cpu_sample(ps[0], 400, budget_s=float(os.environ.get("PG_CPU_BUDGET_S", "15")))
+        cpu = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "port",
+               "sample": f"{done} steps of ensemble disk 0 ({ps[0].imax}x{ps[0].jmax}) in {el:.1f} s"}
+    bytes_cell = 2 * 2 * 3 * (4 * n32 + 8 * (n - n32)) / n    # 2 sweeps x (3 fields in + out), mean width
+    peak, peak_kind = _peaks()
+    achieved = value * bytes_cell / 1e9
+    line = {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": 1,
+        "steps": max_steps, "warmup": 3, "ms_per_step": 1e3 * dev_s / max_steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": f"mixed: f32 planes for {n32} disks, f64 for {n - n32}",
+        "data": "synthetic seeded disks (no public dataset)",
+        "config": {"workload": f"batched ensemble of {n} 2D disks, {orbits:g} orbits each (configs[3])",
+                   "cells": sum(E.disk_cells(p) for p in ps), "fp32_disks": n32,
+                   "policy": f"FP32 planes when q/h^3 <= {E.THERMAL_MASS_FP32}",
+                   "l2": "working set larger than L2", "tuned_shape": None},
+        "vs_plain_fp64_256x768": value / plain, "plain_fp64_256x768": plain,
+        "roofline": {"bound": "hbm", "kernel": "whole batched step", "achieved": achieved, "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "bytes_per_cell_update": bytes_cell},
+        "cpu_baseline": cpu,
+        "e2e": {"value": all_updates / e2e_el, "unit": "zone-updates/s",
+                "h2d_bytes_per_step": dump_bytes / max_steps, "d2h_bytes_per_step": dump_bytes / max_steps,
+                "path": "pg_create + pg_load_rings from host dumps, pg_batch tune/advance/status, pg_save_rings"},
+        "gpu_launches": None,
+        "clocks": clk,
+        "bad_status": [i for i, st in enumerate(res.status) if st],
+    }
+    print(json.dumps(line))
+
+
+def bench_serve(args):
+    """Serving: a seeded request stream (90% 2D disks as in the ensemble, 10%
+    3D disks), Poisson arrivals at 1.5x the measured capacity, admission by a
+    150 GB HBM budget; p50/p99 completion latency and aggregate throughput."""
+    import numpy as np
+    import torch
+    import penguin_2_0_b200 as pg
+    from penguin_2_0_b200 import ensemble as E, serving as S
+    torch.cuda.set_device(0)
+    n = int(os.environ.get("PG_SERVE_N", "200"))
+    scale = float(os.environ.get("PG_SERVE_ORBIT_SCALE", "0.1"))
+    slots = int(os.environ.get("PG_SERVE_SLOTS", "64"))
+    reqs = S.draw_stream(n, seed=0, orbits_range=(5.0 * scale, 50.0 * scale))
+    # capacity: the first 16 requests advanced together to completion
+    cal = E.run_ensemble(reqs[:16], chunk=args.chunk)
+    work = [E.disk_cells(p) * st for p, st in zip(reqs[:16], cal.steps)]
+    capacity = cal.zone_updates_per_s / float(np.mean(work))
+    rate = 1.5 * capacity
+    arrivals = S.poisson_arrivals(n, rate, seed=0)
+    clocks = ClockSampler(0)
+    clocks.start()
+    with pg.Server(0, hbm_budget=150 * 10 ** 9, max_slots=slots, chunk=args.chunk) as srv:
+        done = srv.run_trace(reqs, arrivals)
+        rounds = srv.rounds()
+    clk = clocks.stop()
+    total = sum(d["cells"] * d["steps"] for d in done)
+    t_first = min(d["admit_s"] for d in done)
+    makespan = max(d["finish_s"] for d in done) - t_first
+    lat = S.latency_stats(done)
+    line = {
+        "metric": "zone-updates/s; p50/p99 completion latency", "value": total / makespan,
+        "unit": "zone-updates/s", "n_gpus": 1, "steps": rounds * args.chunk, "warmup": 0,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": f"mixed: f32 planes for {sum(p.precision for p in reqs)} of {n} requests",
+        "data": "synthetic seeded request stream (no public dataset)",
+        "config": {"workload": f"serving {n} requests (sample of configs[4]'s 2000), orbits "
+                               f"{5 * scale:g}-{50 * scale:g} (x{scale:g} of 5-50), 10% 3D",
+                   "arrivals": f"Poisson, {rate:.3f}/s = 1.5 x measured capacity {capacity:.3f}/s",
+                   "hbm_budget_gb": 150, "max_slots": slots, "chunk": args.chunk},
+        "latency": lat,
+        "makespan_s": makespan,
+        "timing": "server wall clock (steady_clock) from first admission to last completion",
+        "clocks": clk,
+        "bad_status": [d["id"] for d in done if d["status"] != 0],
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -216,6 +362,10 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ens":
+        return bench_ensemble(args)
+    if args.workload == "serve":
+        return bench_serve(args)
 
     dist, rank, ws = _dist()
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -85,42 +85,71 @@ class EnsembleResult:
 
 
 def run_ensemble(params: list, device: int = 0, chunk: int = 32, tune_steps: int = 0,
-                 keep_dumps: bool = False, max_steps: int = 10 ** 7) -> EnsembleResult:
-    """Advance every disk to its end time in one batch; the clock is the GPU's
-    (CUDA events on the batch stream would need torch; the host waits on the
-    batch at the end, so wall time equals device time up to the final sync)."""
+                 keep_dumps: bool = False, max_steps: int = 10 ** 7, ics: list | None = None,
+                 on_start=None, on_stop=None, round_chunks: int = 4) -> EnsembleResult:
+    """Advance every disk to its end time in one batch.
+
+    Members whose clock halted (end time reached) leave the batch after each
+    round of `round_chunks` graph replays, so the remaining members' launches
+    carry no idle tiles.  on_start(batch) / on_stop(batch) are called right
+    before the first and after the last timed round (the caller records its
+    CUDA events on batch.stream_ptr()); `seconds` is the host wall time of
+    the same region.  Steps taken by the tuner come before it and are not
+    counted in cell_updates."""
+    if ics is None:
+        ics = [host.build_ic(p) for p in params]
     runs = []
-    for p in params:
-        r = host.Run(p, device).load(host.build_ic(p))
+    for p, ic in zip(params, ics):
+        r = host.Run(p, device).load(ic)
         r.clock_reset(0)
         runs.append(r)
     res = EnsembleResult(params=list(params))
+    n = len(runs)
+    steps = [0] * n
+    simtime = [0.0] * n
+    status = [0] * n
     with host.Batch(device) as b:
         for r in runs:
             b.add(r)
         if tune_steps:
             b.tune(tune_steps)
+        base = [s["ncycle"] for s in b.status()]
         b.sync()
-        st0 = b.status()
+        if on_start:
+            on_start(b)
         t0 = time.perf_counter()
+        live = list(range(n))
         left = max_steps
-        while left > 0:
-            n = min(left, 50 * chunk)
-            b.advance(n, chunk=chunk)
+        while live and left > 0:
+            k = min(left, round_chunks * chunk)
+            b.advance(k, chunk=chunk)
+            left -= k
             st = b.status()
-            left -= n
-            if all(s["halted"] for s in st):
-                break
+            still = []
+            for pos, idx in enumerate(live):
+                s = st[pos]
+                if s["halted"]:
+                    steps[idx], simtime[idx], status[idx] = int(s["ncycle"]), float(s["simtime"]), int(s["status"])
+                    b.remove(runs[idx])
+                else:
+                    still.append(idx)
+            live = still
+        if live:
+            st = b.status()
+            for pos, idx in enumerate(live):
+                s = st[pos]
+                steps[idx], simtime[idx], status[idx] = int(s["ncycle"]), float(s["simtime"]), int(s["status"])
         b.sync()
+        if on_stop:
+            on_stop(b)
         res.seconds = time.perf_counter() - t0
-        st = b.status()
-        for r in list(runs):
-            b.remove(r)
-    for p, s0, s, r in zip(params, st0, st, runs):
-        res.steps.append(int(s["ncycle"]))
-        res.simtime.append(float(s["simtime"]))
-        res.status.append(int(s["status"]))
-        res.cell_updates += disk_cells(p) * int(s["ncycle"] - s0["ncycle"])
+        for idx in live:
+            b.remove(runs[idx])
+    for i, (p, r) in enumerate(zip(params, runs)):
+        res.steps.append(steps[i])
+        res.simtime.append(simtime[i])
+        res.status.append(status[i])
+        res.cell_updates += disk_cells(p) * (steps[i] - base[i])
         if keep_dumps:
             res.dumps.append(r.save())
         r.close()

@@ -331,19 +331,20 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_y(Tables T, Planes P, Phys p
 // v <- v_r, w <- r sin(theta) v_phi (so get_fz's w^2 cos/(r sin)^3 is the
 // centrifugal term); viscosity follows device_viscosity_p's pattern on the
 // arc length r*theta.
-template <int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_sweep_z(Tables T, Planes P, Phys ph, SweepCtl ctl, int ntop, int l0) {
-  __shared__ ChunkShmT<NT> S;
-  StepIn st;
-  if (!load_step(ctl, st)) return;
-  const int n = threadIdx.x;
-  const int i = blockIdx.x, j0 = blockIdx.y, l = blockIdx.z + l0;
+//
+// One pencil chunk: ring i, column j0, chunk l; n is this thread's cell in
+// the chunk and `store` false computes without storing (padding pencils of
+// the packed kernel).
+template <int NT>
+__device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store, const Tables &T, const Planes &P,
+                                             const Phys &ph, const SweepCtl &ctl, const StepIn &st, int ntop,
+                                             int i, int j0, int l) {
   const int nphi = T.nphi, nrg = T.nrg, nk = T.nk;
   const int row = i + NPAD;
   const bool last = (l == T.cz.loop - 1);
   if (last && T.cz.stuck) {
     int k = REAL * l + n;
-    if (n < REAL && k < nk) {
+    if (store && n < REAL && k < nk) {
       size_t idx = ((size_t)k * nrg + row) * nphi + j0;
       int inc = ctl.shift ? T.inc_j[k * nrg + row] : 0;
       size_t o = ((size_t)k * nrg + row) * nphi + wrapm(j0 + inc, nphi);
@@ -430,7 +431,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_z(Tables T, Planes P, Phys p
     __syncthreads();
     if (n >= NPAD && n < lim - NPAD) { S.u[n] = ddu; S.v[n] = ddv; }
   }
-  if (n >= NPAD && n < lim - NPAD) {
+  if (store && n >= NPAD && n < lim - NPAD) {
     // the polar sweep is the last of a 3D step: the FARGO integer shift of
     // each layer (rotate_rings, ppm.cu:309-322) is applied at this store
     int inc = ctl.shift ? T.inc_j[kr * nrg + row] : 0;
@@ -440,6 +441,38 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_z(Tables T, Planes P, Phys p
     P.uo[o] = S.v[n];
     P.vo[o] = S.w[n] / rad_cyl;
   }
+}
+
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sweep_z(Tables T, Planes P, Phys ph, SweepCtl ctl, int ntop, int l0) {
+  __shared__ ChunkShmT<NT> S;
+  StepIn st;
+  if (!load_step(ctl, st)) return;
+  sweep_z_body<NT>(S, threadIdx.x, true, T, P, ph, ctl, st, ntop, blockIdx.x, blockIdx.y, blockIdx.z + l0);
+}
+
+// Polar sweep of single-chunk pencils (nk <= PZ_LIM - 12, the usual 3D
+// disk): PACK pencils of lim = nk + 12 cells share a CTA of PACK * lim
+// threads instead of one pencil per CTA of 32/64 threads with idle lanes.
+// Measured on the 128x1024x32 disk: 4 pencils per CTA at 5 CTAs/SM (56
+// registers) take the polar sweep from 1.85 to 1.30 ms (8 per CTA at 2
+// CTAs/SM: 1.63 ms).  Thread t works on cell t / PACK of pencil t % PACK,
+// and the PACK pencils of a CTA are consecutive azimuth columns of a ring,
+// so a warp's loads of one layer cover PACK adjacent doubles.  Pencils past
+// the last column repeat the last one without storing.
+constexpr int PZ_LIM = 56;
+template <int PACK, int MINB>
+__global__ void __launch_bounds__(PACK * PZ_LIM, MINB) k_sweep_z_packed(Tables T, Planes P, Phys ph, SweepCtl ctl,
+                                                                        int ntop) {
+  __shared__ ChunkShmT<PZ_LIM> S[PACK];
+  StepIn st;
+  if (!load_step(ctl, st)) return;
+  const int p = threadIdx.x % PACK, n = threadIdx.x / PACK;
+  const int npen = T.nr * T.nphi;
+  int col = blockIdx.x * PACK + p;
+  const bool store = col < npen;
+  if (!store) col = npen - 1;
+  sweep_z_body<PZ_LIM>(S[p], n, store, T, P, ph, ctl, st, ntop, col / T.nphi, col % T.nphi, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -1016,6 +1049,11 @@ void sweep_y(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c
 
 void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s) {
   const Chunking &ch = T.cz;
+  if (T.zpack && ch.loop == 1 && !ch.stuck && ch.lim_last <= PZ_LIM) {
+    int npen = T.nr * T.nphi;
+    k_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
+    return;
+  }
   int full = ch.stuck ? ch.loop : ch.loop - 1;
   if (full > 0) {
     dim3 grid(T.nr, T.nphi, full);

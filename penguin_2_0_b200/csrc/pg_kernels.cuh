@@ -28,6 +28,7 @@ __host__ __device__ inline Chunking make_chunking(int n) {
 struct Tables {
   int nr, nphi, nk, nrg;
   int occ8;                                     // 128-thread sweeps capped at 64 registers (8 CTAs/SM)
+  int zpack;                                    // polar pencils per CTA when nk is one chunk (0: one per CTA)
   Chunking cx, cy, cz;
   const double *rx, *rdx, *rxvol, *rxc;         // [nrg]
   const double *radc, *cs2, *nu;                // [nk*nrg]

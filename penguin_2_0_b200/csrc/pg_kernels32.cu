@@ -326,20 +326,18 @@ __global__ void __launch_bounds__(NT, MINB) k32_sweep_y(Tables T, Planes32 P, Ph
 }
 
 // ---------------------------------------------------------------------------
-template <int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k32_sweep_z(Tables T, Planes32 P, Phys ph, SweepCtl ctl, int ntop,
-                                                        int l0) {
-  __shared__ ChunkShm32<NT> S;
-  StepIn32 st;
-  if (!load_step32(ctl, st)) return;
-  const int n = threadIdx.x;
-  const int i = blockIdx.x, j0 = blockIdx.y, l = blockIdx.z + l0;
+// One polar pencil chunk (ring i, column j0, chunk l), cell n of it; with
+// `store` false the pencil is computed and not stored.
+template <int NT>
+__device__ __forceinline__ void sweep_z32_body(ChunkShm32<NT> &S, int n, bool store, const Tables &T,
+                                               const Planes32 &P, const Phys &ph, const SweepCtl &ctl,
+                                               const StepIn32 &st, int ntop, int i, int j0, int l) {
   const int nphi = T.nphi, nrg = T.nrg, nk = T.nk;
   const int row = i + NPAD;
   const bool last = (l == T.cz.loop - 1);
   if (last && T.cz.stuck) {
     int k = REAL * l + n;
-    if (n < REAL && k < nk) {
+    if (store && n < REAL && k < nk) {
       size_t idx = ((size_t)k * nrg + row) * nphi + j0;
       int inc = ctl.shift ? T.inc_j[k * nrg + row] : 0;
       size_t o = ((size_t)k * nrg + row) * nphi + wrapmf(j0 + inc, nphi);
@@ -426,7 +424,7 @@ __global__ void __launch_bounds__(NT, MINB) k32_sweep_z(Tables T, Planes32 P, Ph
     __syncthreads();
     if (n >= NPAD && n < lim - NPAD) { S.u[n] = ddu; S.v[n] = ddv; }
   }
-  if (n >= NPAD && n < lim - NPAD) {
+  if (store && n >= NPAD && n < lim - NPAD) {
     int rkk = kr * nrg + row;
     int inc = ctl.shift ? T.inc_j[rkk] : 0;
     size_t o = (size_t)rkk * nphi + wrapmf(j0 + inc, nphi);
@@ -435,6 +433,31 @@ __global__ void __launch_bounds__(NT, MINB) k32_sweep_z(Tables T, Planes32 P, Ph
     P.uo[o] = S.v[n];
     P.vo[o] = (float)(S.L[n] / rad_cyl - vbg);
   }
+}
+
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k32_sweep_z(Tables T, Planes32 P, Phys ph, SweepCtl ctl, int ntop,
+                                                        int l0) {
+  __shared__ ChunkShm32<NT> S;
+  StepIn32 st;
+  if (!load_step32(ctl, st)) return;
+  sweep_z32_body<NT>(S, threadIdx.x, true, T, P, ph, ctl, st, ntop, blockIdx.x, blockIdx.y, blockIdx.z + l0);
+}
+
+// single-chunk polar pencils packed 4 per CTA (see k_sweep_z_packed)
+constexpr int PZ32_LIM = 56;
+template <int PACK, int MINB>
+__global__ void __launch_bounds__(PACK * PZ32_LIM, MINB) k32_sweep_z_packed(Tables T, Planes32 P, Phys ph,
+                                                                            SweepCtl ctl, int ntop) {
+  __shared__ ChunkShm32<PZ32_LIM> S[PACK];
+  StepIn32 st;
+  if (!load_step32(ctl, st)) return;
+  const int p = threadIdx.x % PACK, n = threadIdx.x / PACK;
+  const int npen = T.nr * T.nphi;
+  int col = blockIdx.x * PACK + p;
+  const bool store = col < npen;
+  if (!store) col = npen - 1;
+  sweep_z32_body<PZ32_LIM>(S[p], n, store, T, P, ph, ctl, st, ntop, col / T.nphi, col % T.nphi, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -610,6 +633,11 @@ void sweep_y32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCt
 
 void sweep_z32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s) {
   const Chunking &ch = T.cz;
+  if (T.zpack && ch.loop == 1 && !ch.stuck && ch.lim_last <= PZ32_LIM) {
+    int npen = T.nr * T.nphi;
+    k32_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
+    return;
+  }
   int full = ch.stuck ? ch.loop : ch.loop - 1;
   if (full > 0) {
     dim3 grid(T.nr, T.nphi, full);

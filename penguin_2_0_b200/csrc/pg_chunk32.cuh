@@ -20,6 +20,11 @@
 //  * Lagrangian face positions are kept as displacements delx from the
 //    Eulerian faces (widths dx = dx0 + delx[n+1] - delx[n]), so FP32 does not
 //    lose the small face motions against face coordinates of order 1;
+//  * mass moves in FP64: displacements, Lagrangian widths and volumes, the
+//    remap's interface coefficients, the density parabola and the swept
+//    masses.  In a steady flow (the gas bound to a planet) the same large
+//    fluxes cross the same faces every step, and FP32 rounding of them would
+//    repeat and add up step after step;
 //  * forces, geometry factors and positions are evaluated in FP64 from the
 //    FP64 face coordinate of each cell.
 #pragma once
@@ -36,12 +41,14 @@ struct ChunkShm32 {
   float r[NT + 2], p[NT + 2], u[NT + 2], v[NT + 2], w[NT + 2], dx0[NT + 2];
   float q[NT + 2], dx[NT + 2], umid[NT + 2], pmid[NT + 2], tmp1[NT + 2], dl[NT + 2];
   double L[NT + 2], Lal[NT + 2], Lda[NT + 2], La6[NT + 2], Lflux[NT + 2], xa0[NT + 2];
+  double Rd[NT + 2], dld[NT + 2];   // FP64 Lagrangian density and face displacements
 };
 
 struct CellIn32 {
   double rad, azi, pol, vrot, dvol0;
   double omres;   // azimuthal sweep: v_bg / r_cyl - v_rot - FrRot (FP64)
   double sig;     // this cell's Sigma in FP64 (S_bg + dS)
+  double dx0;     // this cell's Eulerian width in FP64
 };
 
 __device__ __forceinline__ float min3f(float A, float B, float C) {
@@ -287,18 +294,21 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
     else delx = dt * (double)S.umid[n] / c.rad;
     dtdm = (float)(dt / ((double)S.r[n] * c.dvol0));
     S.dl[n] = (float)delx;
+    S.dld[n] = delx;
   }
   __syncthreads();
   double xa = xa0n;
   float dxl = 0.f;
+  double dxld = 0.0;
   if (n >= 3 && n < nmax - 3) {
     dxl = S.dx0[n] + (S.dl[n + 1] - S.dl[n]);
     S.dx[n] = dxl;
-    xa = xa0n + (double)S.dl[n];
+    dxld = c.dx0 + (S.dld[n + 1] - S.dld[n]);
+    xa = xa0n + S.dld[n];
   }
   __syncthreads();
   if (n >= 3 && n < nmax - 3) {
-    double xcl = xa + 0.5 * (double)dxl;
+    double xcl = xa + 0.5 * dxld;
     double a1, a2;
     if (AXIS == 0) {
       a1 = centre_force32<0, SPH>(n, 0.0, c.rad, c.azi, c.pol, S.L, S.w, pl, ph);
@@ -317,8 +327,8 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
   if (n >= 3 && n < nmax - 2) {
     // as in the reference, the last cell of this range keeps xa = xa0
     // (evolve.cu:36-44 sets xa for n < nmax-3 only)
-    double dxn = S.dx[n];
-    double d = (n < nmax - 3) ? (double)S.dl[n] : 0.0;
+    double dxn = (n < nmax - 3) ? dxld : (double)S.dx[n];
+    double d = (n < nmax - 3) ? S.dld[n] : 0.0;
     if (AXIS == 0) {
       if (!SPH) { dvol = dxn * (xa + 0.5 * dxn); vfac[n] = (float)(xa0n + 0.5 * d); }
       else {
@@ -339,6 +349,7 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
     double rl = c.sig * (c.dvol0 / dvol);
     m_d = c.sig * c.dvol0;   // Lagrangian mass, FP64
     S.r[n] = fmaxf((float)rl, kSmallrF);
+    S.Rd[n] = fmax(rl, (double)kSmallrF);
     float dum = S.u[n];
     float delx = 0.5f * (float)dt * (fto1 + fto2);
     delx += -dtdm * (S.pmid[n + 1] - S.pmid[n]) * 0.5f * (vfac[n + 1] + vfac[n]);
@@ -348,7 +359,7 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
   // ---- remap ----
   al = S.tmp1; da = S.umid; a6 = S.pmid;
   paraset32(n, 3, nmax - 3, par, S.dx, al, da, a6);
-  double dd = (n >= 3 && n < nmax - 3) ? (double)S.dl[n] : 0.0;
+  double dd = (n >= 3 && n < nmax - 3) ? S.dld[n] : 0.0;
   double lvol;
   if (AXIS == 0) {
     if (!SPH) lvol = dd * (xa0n + 0.5 * dd);
@@ -358,32 +369,38 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
   } else {
     lvol = 2.0 * sin(xa0n + 0.5 * dd) * sin(0.5 * dd) * c.rad;
   }
-  float dxf = (float)dd;
-  const bool delC = (dxf >= 0.f);
-  parabola32<float>(n, 3, nmax - 3, flat, S.r, al, da, a6, par);
+  const bool delC = (dd >= 0.0);
   float *flux = S.dx;
-  float dxnn = 0.f, dxnm = 0.f;
-  if (n >= 6 && n < nmax - 5) { dxnn = S.dx[n]; dxnm = S.dx[n - 1]; }
+  // FP64 mass transport: Lagrangian widths, interface coefficients, density
+  // parabola and the swept mass of each face (the L slots are free here)
+  double *dxd = S.Lflux;
+  if (n >= 3 && n < nmax - 3) dxd[n] = dxld;
   __syncthreads();
-  float dxf2 = 0.f, fr = 0.f;
+  Par pd;
+  paraset(n, 3, nmax - 3, pd, dxd, S.Lal, S.Lda, S.La6);
+  double dxnn = 0.0, dxnm = 0.0;
+  if (n >= 6 && n < nmax - 5) { dxnn = dxd[n]; dxnm = dxd[n - 1]; }
+  parabola(n, 3, nmax - 3, (double)flat, S.Rd, S.Lal, S.Lda, S.La6, pd);
+  double xd = 0.0, x2d = 0.0, frd = 0.0;
   if (n >= 6 && n < nmax - 5) {
     if (delC) {
-      dxf = 0.5f * dxf / dxnm;
-      dxf2 = 1.0f - kFourthdF * dxf;
-      fr = (al[n - 1] + da[n - 1] - dxf * (da[n - 1] - dxf2 * a6[n - 1])) * (float)lvol;
+      xd = 0.5 * dd / dxnm;
+      x2d = 1.0 - kFourthd * xd;
+      frd = (S.Lal[n - 1] + S.Lda[n - 1] - xd * (S.Lda[n - 1] - x2d * S.La6[n - 1])) * lvol;
     } else {
-      dxf = 0.5f * dxf / dxnn;
-      dxf2 = 1.0f + kFourthdF * dxf;
-      fr = (al[n] - dxf * (da[n] + dxf2 * a6[n])) * (float)lvol;
+      xd = 0.5 * dd / dxnn;
+      x2d = 1.0 + kFourthd * xd;
+      frd = (S.Lal[n] - xd * (S.Lda[n] + x2d * S.La6[n])) * lvol;
     }
-    flux[n] = fr;
+    S.Lflux[n] = frd;
   }
   __syncthreads();
+  const float fr = (float)frd, dxf = (float)xd, dxf2 = (float)x2d;
   float mm = 0.f, invm = 0.f;
   double mnew_d = 1.0, sig_new = c.sig;
   if (n >= 6 && n < nmax - 6) {
     mm = S.r[n] * (float)dvol;
-    mnew_d = m_d + (double)fr - (double)flux[n + 1];
+    mnew_d = m_d + frd - S.Lflux[n + 1];
     sig_new = fmax((double)kSmallrF, mnew_d / c.dvol0);
     S.r[n] = (float)sig_new;
     invm = 1.0f / (S.r[n] * (float)c.dvol0);
@@ -400,11 +417,11 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
   remap_f(S.u);
   if (hasL) {
     // FP64 angular momentum: L_new = (L m + F_n - F_{n+1}) / (m + f_n - f_{n+1})
-    parabola32<double>(n, 3, nmax - 3, flat, S.L, S.Lal, S.Lda, S.La6, par);
+    __syncthreads();   // every thread has read the mass flux of face n+1
+    parabola(n, 3, nmax - 3, (double)flat, S.L, S.Lal, S.Lda, S.La6, pd);
     if (n >= 6 && n < nmax - 5) {
-      double x = dxf, x2 = dxf2;
-      if (delC) S.Lflux[n] = (S.Lal[n - 1] + S.Lda[n - 1] - x * (S.Lda[n - 1] - x2 * S.La6[n - 1])) * (double)fr;
-      else      S.Lflux[n] = (S.Lal[n] - x * (S.Lda[n] + x2 * S.La6[n])) * (double)fr;
+      if (delC) S.Lflux[n] = (S.Lal[n - 1] + S.Lda[n - 1] - xd * (S.Lda[n - 1] - x2d * S.La6[n - 1])) * frd;
+      else      S.Lflux[n] = (S.Lal[n] - xd * (S.Lda[n] + x2d * S.La6[n])) * frd;
     }
     __syncthreads();
     if (n >= 6 && n < nmax - 6) S.L[n] = (S.L[n] * m_d + (S.Lflux[n] - S.Lflux[n + 1])) / mnew_d;

@@ -105,6 +105,7 @@ __device__ __forceinline__ void sweep_x32_body(ChunkShm32<NT> &S, const Tables &
     c.vrot = T.res_v[rk] / rad_cyl;
     S.xa0[n] = T.rx[row];
     S.dx0[n] = (float)T.rdx[row];
+    c.dx0 = T.rdx[row];
     c.sig = sbg + (double)P.r[idx];
     float r = (float)c.sig;
     S.r[n] = r;
@@ -259,6 +260,7 @@ __device__ __forceinline__ void sweep_y32_body(ChunkShm32<NT> &S, double *red, c
       c.dvol0 = dvol0;
       S.xa0[n] = xa0;
       S.dx0[n] = (float)T.dy[j0];
+      c.dx0 = T.dy[j0];
       c.sig = sbg + (double)P.r[s];
       float r = (float)c.sig;
       S.r[n] = r;
@@ -394,6 +396,7 @@ __device__ __forceinline__ void sweep_z32_body(ChunkShm32<NT> &S, int n, bool st
     c.dvol0 = zvol * rad;
     S.xa0[n] = za;
     S.dx0[n] = (float)dz;
+    c.dx0 = dz;
     S.r[n] = r; S.p[n] = p;
     S.u[n] = w;        // v_theta
     S.v[n] = u;        // v_r

@@ -1,11 +1,12 @@
 """Benchmark of the hydro step: zone-updates/s on one or more B200s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cfg1|cfg0|cfg2|big|prof]
+                    [--workload cfg1|cfg0|cfg2|cfg2_fp64|cfg0_fp32|ens|serve|big|prof|prof32]
 
 Default workload: the 3D spherical disk of 128 x 1024 x 32 (4.19 M cells),
 the plain FP64 method on which the metric is quoted; cfg0 is the 2D
-256 x 768 disk, cfg2 the 2D 1024 x 3072 grid.
+256 x 768 disk, cfg2 the 2D 1024 x 3072 grid with FP32 planes, ens the batched
+ensemble of 64 disks (10 orbits each), serve the serving-loop stream.
 
 A step is one full time step of the disk (get_dt, FARGO shift, planet kick,
 all directional sweeps, damping, drift/kick, diagnostics) over the whole
@@ -24,10 +25,12 @@ as one region.
 roofline: the dominant kernel's algorithmic bytes (3 fields read + 3 written
 in FP64 = 48 B per cell per 2D sweep, 4 fields = 64 B in 3D) over its mean
 event-timed duration, against MEASURED_PEAKS.json's HBM copy bandwidth.
-e2e: the same metric through the reference-facing calls of the C ABI
-(pg_get_dt, pg_index_shift, pg_sweep2d, pg_damp, pg_reduce: host syncs as in
-main.cu), with the step's scalars (dt, planet, FrRot) going to the device
-and dt, mass and torque coming back every step.
+e2e: the same metric through the reference-facing calls of the C ABI: the
+seeded dump is loaded from pinned host memory (pg_load_rings), the steps run
+through pg_get_dt, pg_index_shift, pg_sweep2d/3d, pg_damp and pg_reduce with
+main.cu's host syncs (dt, planet and FrRot to the device, dt, mass and torque
+back every step), and the final dump is saved to pinned host memory, all
+inside the timed region.
 cpu_baseline: the CPU oracle (a restatement of the reference's sweeps in C,
 OpenMP over the box's cores) on a bounded sample of the same workload.
 """
@@ -246,6 +249,7 @@ def bench_ensemble(args):
         e = torch.cuda.Event(enable_timing=True)
         e.record(torch.cuda.ExternalStream(b.stream_ptr()))
         ev["a"] = e
+        ev["l0"] = b.launches()
         clocks.start()
 
     def on_stop(b):
@@ -253,6 +257,7 @@ def bench_ensemble(args):
         e.record(torch.cuda.ExternalStream(b.stream_ptr()))
         e.synchronize()
         ev["b"] = e
+        ev["l1"] = b.launches()
 
     t0 = time.perf_counter()
     res = E.run_ensemble(ps, ics=ics, chunk=args.chunk, tune_steps=2, keep_dumps=True,
@@ -291,7 +296,7 @@ def bench_ensemble(args):
         "e2e": {"value": all_updates / e2e_el, "unit": "zone-updates/s",
                 "h2d_bytes_per_step": dump_bytes / max_steps, "d2h_bytes_per_step": dump_bytes / max_steps,
                 "path": "pg_create + pg_load_rings from host dumps, pg_batch tune/advance/status, pg_save_rings"},
-        "gpu_launches": None,
+        "gpu_launches": int(ev["l1"] - ev["l0"]),
         "clocks": clk,
         "bad_status": [i for i, st in enumerate(res.status) if st],
     }
@@ -459,19 +464,30 @@ def main():
             if line.startswith("traffic_bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
 
-    # e2e through the reference-facing calls (host-driven loop, host syncs)
+    # e2e through the reference-facing calls: the dump goes in from pinned host
+    # memory (pg_load_rings), the host-driven loop runs with the reference's
+    # syncs (dt, planet and FrRot to the device, dt, mass and torque back every
+    # step), and the final dump comes back (pg_save_rings), all timed
+    import numpy as np
     e2e_steps = max(3, min(args.steps // 10, 200))
+    dump_bytes = len(ic)
+    pin_in = torch.empty(dump_bytes, dtype=torch.uint8, pin_memory=True)
+    pin_in.numpy()[:] = np.frombuffer(bytes(ic), dtype=np.uint8)
+    pin_out = torch.empty(dump_bytes, dtype=torch.uint8, pin_memory=True)
     run2 = pg.Run(p, local).load(ic)
     run2.kernel_loop(2)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
 
     def rec(s, simtime, dt_used, planet, FrRot):
         pg.GPU_output_reduction(run2, planet, 0.0, 0)
         if p.plnt_flag:
             pg.GPU_output_reduction(run2, planet, 0.0, 9)
 
+    _barrier(dist)
+    t0 = time.perf_counter()
+    run2.load_from(pin_in.data_ptr(), dump_bytes)
     run2.kernel_loop(e2e_steps, record=rec)
+    run2.save_to(pin_out.data_ptr(), dump_bytes)
     torch.cuda.synchronize()
     e2e_el = _max_over_ranks(dist, time.perf_counter() - t0)
     e2e_value = cells * e2e_steps * ws / e2e_el
@@ -499,9 +515,12 @@ def main():
                          "traffic": traffic, "bytes_per_launch": bytes_per_launch,
                          "mean_launch_ms": mean[top], "kernels_ms": mean},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": 64 + 16,
-                    "d2h_bytes_per_step": 8 + 8 + 8,
-                    "path": "host loop over pg_get_dt/pg_index_shift/pg_sweep2d/pg_damp/pg_reduce"},
+            "e2e": {"value": e2e_value, "unit": "zone-updates/s",
+                    "h2d_bytes_per_step": (dump_bytes + (64 + 16) * e2e_steps) / e2e_steps,
+                    "d2h_bytes_per_step": (dump_bytes + (8 + 8 + 8) * e2e_steps) / e2e_steps,
+                    "steps": e2e_steps,
+                    "path": "pg_load_rings from pinned host memory, host loop over pg_get_dt/pg_index_shift/"
+                            "pg_sweep2d|3d/pg_damp/pg_reduce, pg_save_rings to pinned host memory"},
             "gpu_launches": int(launches),
             "clocks": clk,
         }

@@ -172,6 +172,15 @@ class Run:
         _check(_lib.lib().pg_load_rings(self._h, cbuf, n), self, "pg_load_rings")
         return self
 
+    def load_from(self, ptr: int, nbytes: int) -> "Run":
+        """pg_load_rings from a raw host pointer (e.g. a pinned buffer)."""
+        _check(_lib.lib().pg_load_rings(self._h, C.c_void_p(ptr), nbytes), self, "pg_load_rings")
+        return self
+
+    def save_to(self, ptr: int, nbytes: int):
+        """pg_save_rings into a raw host pointer (e.g. a pinned buffer)."""
+        _check(_lib.lib().pg_save_rings(self._h, C.c_void_p(ptr), nbytes), self, "pg_save_rings")
+
     def load_dump(self, path: str) -> "Run":
         _check(_lib.lib().pg_load_dump(self._h, path.encode()), self, "pg_load_dump")
         return self

@@ -75,15 +75,15 @@ __device__ __forceinline__ bool load_step(const SweepCtl &c, StepIn &s) {
 // One radial pencil chunk: column j0, chunk l, polar layer k.  The body is
 // shared by the per-run kernel and the batched kernels of pg_batch.cu.
 template <bool SPH, bool THREED, int NT>
-__device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, const Tables &T, const Planes &P, const Phys &ph,
-                                             const SweepCtl &ctl, const StepIn &st, int j0, int l, int k) {
-  const int n = threadIdx.x;
+__device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, int n, bool store, const Tables &T, const Planes &P,
+                                             const Phys &ph, const SweepCtl &ctl, const StepIn &st, int j0, int l,
+                                             int k) {
   const bool last = (l == T.cx.loop - 1);
   const int nphi = T.nphi, nrg = T.nrg;
   if (last && T.cx.stuck) {
     // ppm.cu:48 gives this chunk lim = 12: its rings keep their values
     int i = REAL * l + n;
-    if (n < REAL && i < T.nr) {
+    if (store && n < REAL && i < T.nr) {
       size_t idx = ((size_t)k * nrg + i + NPAD) * nphi + j0;
       P.ro[idx] = P.r[idx]; P.uo[idx] = P.u[idx]; P.vo[idx] = P.v[idx];
       if (THREED) P.wo[idx] = P.w[idx];
@@ -152,7 +152,7 @@ __device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, const Tables &T, 
       if (THREED) S.w[n] = ddw;
     }
   }
-  if (n >= NPAD && n < lim - NPAD) {
+  if (store && n >= NPAD && n < lim - NPAD) {
     P.ro[idx] = S.r[n];
     P.uo[idx] = S.u[n];
     P.vo[idx] = S.v[n] / rad_cyl;
@@ -165,7 +165,26 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_x(Tables T, Planes P, Phys p
   __shared__ ChunkShmT<NT> S;
   StepIn st;
   if (!load_step(ctl, st)) return;
-  sweep_x_body<SPH, THREED, NT>(S, T, P, ph, ctl, st, blockIdx.x, blockIdx.y + l0, blockIdx.z);
+  sweep_x_body<SPH, THREED, NT>(S, threadIdx.x, true, T, P, ph, ctl, st, blockIdx.x, blockIdx.y + l0, blockIdx.z);
+}
+
+// The short last chunk of radial pencils (lim <= 64 cells): 4 adjacent
+// columns share a CTA of 4 * lim threads, thread t on cell t / 4 of column
+// t % 4 (a warp's loads of one ring cover 4 adjacent doubles), instead of one
+// column per 32/64-thread CTA with idle lanes.  Columns past the last one
+// repeat it without storing.
+constexpr int PX_LIM = 64;
+template <bool SPH, bool THREED, int MINB>
+__global__ void __launch_bounds__(4 * PX_LIM, MINB) k_sweep_x_packed(Tables T, Planes P, Phys ph, SweepCtl ctl) {
+  __shared__ ChunkShmT<PX_LIM> S[4];
+  StepIn st;
+  if (!load_step(ctl, st)) return;
+  const int p = threadIdx.x & 3, n = threadIdx.x >> 2;
+  const int npen = T.nphi * T.nk;
+  int col = blockIdx.x * 4 + p;
+  const bool store = col < npen;
+  if (!store) col = npen - 1;
+  sweep_x_body<SPH, THREED, PX_LIM>(S[p], n, store, T, P, ph, ctl, st, col % T.nphi, T.cx.loop - 1, col / T.nphi);
 }
 
 // ---------------------------------------------------------------------------
@@ -958,7 +977,7 @@ __global__ void __launch_bounds__(128, MINB) kb_sweep_x(BatchQueue q) {
       const int lt = t - q.start[r], nphi = b.T.nphi;
       Planes P = b.PX;
       P.p0 = (b.p0 && b.clk->ncycle == b.p0_cycle) ? b.p0 : nullptr;
-      sweep_x_body<false, false, 128>(S, b.T, P, b.ph, ctl, st, lt % nphi, lt / nphi, 0);
+      sweep_x_body<false, false, 128>(S, threadIdx.x, true, b.T, P, b.ph, ctl, st, lt % nphi, lt / nphi, 0);
     }
     __syncthreads();
   }
@@ -1021,6 +1040,12 @@ void sweep_x(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c
     else PG_LAUNCH_X(false, false, 128, grid, 0);
   }
   if (!ch.stuck) {
+    if (T.zpack && ch.lim_last <= PX_LIM) {
+      int npen = T.nphi * T.nk, blocks = (npen + 3) / 4, nt = 4 * ch.lim_last;
+      if (ndim == 3) k_sweep_x_packed<true, true, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
+      else k_sweep_x_packed<false, false, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
+      return;
+    }
     dim3 grid(T.nphi, 1, T.nk);
     int nt = cta_for(ch.lim_last);
     int l0 = ch.loop - 1;

@@ -72,15 +72,14 @@ __device__ __forceinline__ void derivs_w(T &first, T &second, int n, const float
 // One radial pencil chunk: column j0, chunk l, polar layer k.  The body is
 // shared by the per-run kernel and the batched kernels of pg_batch.cu.
 template <bool SPH, bool THREED, int NT>
-__device__ __forceinline__ void sweep_x32_body(ChunkShm32<NT> &S, const Tables &T, const Planes32 &P,
-                                               const Phys &ph, const SweepCtl &ctl, const StepIn32 &st,
-                                               int j0, int l, int k) {
-  const int n = threadIdx.x;
+__device__ __forceinline__ void sweep_x32_body(ChunkShm32<NT> &S, int n, bool store, const Tables &T,
+                                               const Planes32 &P, const Phys &ph, const SweepCtl &ctl,
+                                               const StepIn32 &st, int j0, int l, int k) {
   const bool last = (l == T.cx.loop - 1);
   const int nphi = T.nphi, nrg = T.nrg;
   if (last && T.cx.stuck) {
     int i = REAL * l + n;
-    if (n < REAL && i < T.nr) {
+    if (store && n < REAL && i < T.nr) {
       size_t idx = ((size_t)k * nrg + i + NPAD) * nphi + j0;
       P.ro[idx] = P.r[idx]; P.uo[idx] = P.u[idx]; P.vo[idx] = P.v[idx];
       if (THREED) P.wo[idx] = P.w[idx];
@@ -156,7 +155,7 @@ __device__ __forceinline__ void sweep_x32_body(ChunkShm32<NT> &S, const Tables &
       if (THREED) S.w[n] = ddw;
     }
   }
-  if (n >= NPAD && n < lim - NPAD) {
+  if (store && n >= NPAD && n < lim - NPAD) {
     P.ro[idx] = (float)(sig - sbg);
     P.uo[idx] = S.u[n];
     P.vo[idx] = (float)(S.L[n] / rad_cyl - vbg);
@@ -169,7 +168,26 @@ __global__ void __launch_bounds__(NT, MINB) k32_sweep_x(Tables T, Planes32 P, Ph
   __shared__ ChunkShm32<NT> S;
   StepIn32 st;
   if (!load_step32(ctl, st)) return;
-  sweep_x32_body<SPH, THREED, NT>(S, T, P, ph, ctl, st, blockIdx.x, blockIdx.y + l0, blockIdx.z);
+  sweep_x32_body<SPH, THREED, NT>(S, threadIdx.x, true, T, P, ph, ctl, st, blockIdx.x, blockIdx.y + l0,
+                                  blockIdx.z);
+}
+
+// short last chunks of radial pencils packed 4 columns per CTA (see
+// k_sweep_x_packed)
+constexpr int PX32_LIM = 64;
+template <bool SPH, bool THREED, int MINB>
+__global__ void __launch_bounds__(4 * PX32_LIM, MINB) k32_sweep_x_packed(Tables T, Planes32 P, Phys ph,
+                                                                         SweepCtl ctl) {
+  __shared__ ChunkShm32<PX32_LIM> S[4];
+  StepIn32 st;
+  if (!load_step32(ctl, st)) return;
+  const int p = threadIdx.x & 3, n = threadIdx.x >> 2;
+  const int npen = T.nphi * T.nk;
+  int col = blockIdx.x * 4 + p;
+  const bool store = col < npen;
+  if (!store) col = npen - 1;
+  sweep_x32_body<SPH, THREED, PX32_LIM>(S[p], n, store, T, P, ph, ctl, st, col % T.nphi, T.cx.loop - 1,
+                                        col / T.nphi);
 }
 
 // ---------------------------------------------------------------------------
@@ -556,7 +574,7 @@ __global__ void __launch_bounds__(128, MINB) kb32_sweep_x(BatchQueue q) {
     StepIn32 st;
     if (load_step32(ctl, st)) {
       const int lt = t - q.start[r], nphi = b.T.nphi;
-      sweep_x32_body<false, false, 128>(S, b.T, b.QX, b.ph, ctl, st, lt % nphi, lt / nphi, 0);
+      sweep_x32_body<false, false, 128>(S, threadIdx.x, true, b.T, b.QX, b.ph, ctl, st, lt % nphi, lt / nphi, 0);
     }
     __syncthreads();
   }
@@ -611,6 +629,12 @@ void sweep_x32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCt
     else PG32_X(false, false, 128, grid, 0);
   }
   if (!ch.stuck) {
+    if (T.zpack && ch.lim_last <= PX32_LIM) {
+      int npen = T.nphi * T.nk, blocks = (npen + 3) / 4, nt = 4 * ch.lim_last;
+      if (ndim == 3) k32_sweep_x_packed<true, true, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
+      else k32_sweep_x_packed<false, false, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
+      return;
+    }
     dim3 grid(T.nphi, 1, T.nk);
     int nt = cta_for32(ch.lim_last), l0 = ch.loop - 1;
     if (ndim == 3) PG32_X(true, true, nt, grid, l0);

@@ -57,23 +57,3 @@ def test_3d_fused_loop_equals_host_loop(gpu):
         fa, fb = pg.dump_fields(a.save(), p), pg.dump_fields(b.save(), p)
         for k in ("r", "u", "v", "w", "rot_j"):
             np.testing.assert_array_equal(fa[k], fb[k], err_msg=k)
-
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("kmax,precision", [(16, 0), (24, 0), (16, 1)])
-def test_3d_packed_polar_sweep_is_bitwise(gpu, monkeypatch, kmax, precision):
-    # polar pencils of one chunk run 4 per CTA (default) or 1 per CTA; the
-    # cell arithmetic is the same in both shapes
-    p = _p(kmax=kmax, jmax=132, precision=precision)
-    ic = pg.build_ic(p)
-    out = {}
-    for pack in ("0", "4"):
-        monkeypatch.setenv("PG_POLAR_PACK", pack)
-        with pg.Run(p, 0) as r:
-            r.load(ic)
-            r.clock_reset(0)
-            r.advance(4)
-            out[pack] = pg.dump_fields(r.save(), p)
-    for pack in ("4",):
-        for k in ("r", "u", "v", "w", "rot_j"):
-            np.testing.assert_array_equal(out[pack][k], out["0"][k], err_msg=f"pack {pack} {k}")

@@ -17,7 +17,11 @@ struct CellIn {
   double pol;    // polar angle (0 in 2D)
   double vrot;   // res_v / rad_cyl of the cell's ring
   double dvol0;  // Eulerian cell volume along the sweep
+  double sinpol; // sin(pol), formed once per cell (radial and azimuthal sweeps in 3D)
 };
+
+// x^2 where the reference writes pow(x, 2)
+__device__ __forceinline__ double sq(double x) { return x * x; }
 
 template <int AXIS, bool SPH, class SHM>
 __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, const SHM &S,
@@ -31,20 +35,20 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
       if (ph.plnt) { grav = grav_rad_cyl(rad, azi, c.pol, pl, hdt); grav += -1.0 / rad / rad; }
       else { double dis = sqrt(rad * rad + c.pol * c.pol); grav = -rad / dis / dis / dis; }
       double f = grav;
-      f += pow(0.5 * (S.v[n] + S.v[n - 1]), 2) / rad / rad / rad;
+      f += sq(0.5 * (S.v[n] + S.v[n - 1])) / rad / rad / rad;
       ftot = f;
     } else {
-      grav = ph.plnt ? grav_rad_sph(rad, azi, c.pol, pl, hdt) : -1.0 / rad / rad;
+      grav = ph.plnt ? grav_rad_sph_s(rad, azi, c.sinpol, pl, hdt) : -1.0 / rad / rad;
       double f = grav;
-      f += pow(0.5 * (S.w[n] + S.w[n - 1]), 2) / rad / rad / rad;
-      f += pow(0.5 * (S.v[n] + S.v[n - 1]), 2) / rad / pow(rad * sin(c.pol), 2);
+      f += sq(0.5 * (S.w[n] + S.w[n - 1])) / rad / rad / rad;
+      f += sq(0.5 * (S.v[n] + S.v[n - 1])) / rad / sq(rad * c.sinpol);
       ftot = f;
     }
   } else if (AXIS == 1) {
     // get_fy forces.cu:265-296 at xa0[n] + hdt v_rot
     double azi = S.xa0[n] + hdt * c.vrot;
     if (!SPH) ftot = ph.plnt ? grav_azi_cyl(c.rad, azi, c.pol, pl, hdt) : 0.0;
-    else ftot = ph.plnt ? grav_azi_sph(c.rad, azi, c.pol, pl, hdt) : 0.0;
+    else ftot = ph.plnt ? grav_azi_sph_s(c.rad, azi, c.sinpol, pl, hdt) : 0.0;
   } else {
     // get_fz_bound forces.cu:298-334 (ngeomz 5) at the face angle xa0[n]
     double pol = S.xa0[n];
@@ -52,7 +56,7 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
     double grav = ph.plnt ? grav_pol_sph(c.rad, azi, pol, pl, hdt) : 0.0;
     double rad_cyl = c.rad * sin(pol);
     double f = grav;
-    f += (pow(0.5 * (S.w[n] + S.w[n - 1]), 2) * cos(pol)) / rad_cyl / rad_cyl / rad_cyl;
+    f += (sq(0.5 * (S.w[n] + S.w[n - 1])) * cos(pol)) / rad_cyl / rad_cyl / rad_cyl;
     ftot = f;
   }
 }
@@ -60,7 +64,7 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
 // get_fx / get_fy / get_fz at a cell centre (forces.cu:226-372)
 template <int AXIS, bool SPH, class SHM>
 __device__ __forceinline__ double centre_force(int n, double dt, double rad, double azi, double pol,
-                                               const SHM &S, const Body &pl, const Phys &ph) {
+                                               double sinpol, const SHM &S, const Body &pl, const Phys &ph) {
   if (AXIS == 0) {
     double grav;
     if (!SPH) {
@@ -70,15 +74,15 @@ __device__ __forceinline__ double centre_force(int n, double dt, double rad, dou
       f += S.v[n] * S.v[n] / rad / rad / rad;
       return f;
     } else {
-      grav = ph.plnt ? grav_rad_sph(rad, azi, pol, pl, dt) : -1.0 / rad / rad;
+      grav = ph.plnt ? grav_rad_sph_s(rad, azi, sinpol, pl, dt) : -1.0 / rad / rad;
       double f = grav;
       f += S.w[n] * S.w[n] / rad / rad / rad;
-      f += S.v[n] * S.v[n] / rad / pow(rad * sin(pol), 2);
+      f += S.v[n] * S.v[n] / rad / sq(rad * sinpol);
       return f;
     }
   } else if (AXIS == 1) {
     if (!SPH) return ph.plnt ? grav_azi_cyl(rad, azi, pol, pl, dt) : 0.0;
-    return ph.plnt ? grav_azi_sph(rad, azi, pol, pl, dt) : 0.0;
+    return ph.plnt ? grav_azi_sph_s(rad, azi, sinpol, pl, dt) : 0.0;
   } else {
     double grav = ph.plnt ? grav_pol_sph(rad, azi, pol, pl, dt) : 0.0;
     double rad_cyl = rad * sin(pol);
@@ -202,14 +206,14 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   if (n >= 3 && n < nmax - 3) {
     double xcl = xa + 0.5 * S.dx[n];
     if (AXIS == 0) {
-      fto1 = centre_force<0, SPH>(n, 0.0, c.rad, c.azi, c.pol, S, pl, ph);
-      fto2 = centre_force<0, SPH>(n, dt, xcl, c.azi + dt * c.vrot, c.pol, S, pl, ph);
+      fto1 = centre_force<0, SPH>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S, pl, ph);
+      fto2 = centre_force<0, SPH>(n, dt, xcl, c.azi + dt * c.vrot, c.pol, c.sinpol, S, pl, ph);
     } else if (AXIS == 1) {
-      fto1 = centre_force<1, SPH>(n, 0.0, c.rad, c.azi, c.pol, S, pl, ph);
-      fto2 = centre_force<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, S, pl, ph);
+      fto1 = centre_force<1, SPH>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S, pl, ph);
+      fto2 = centre_force<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, c.sinpol, S, pl, ph);
     } else {
-      fto1 = centre_force<2, SPH>(n, 0.0, c.rad, c.azi, c.pol, S, pl, ph);
-      fto2 = centre_force<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, S, pl, ph);
+      fto1 = centre_force<2, SPH>(n, 0.0, c.rad, c.azi, c.pol, 0.0, S, pl, ph);
+      fto2 = centre_force<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, 0.0, S, pl, ph);
     }
   }
   __syncthreads();

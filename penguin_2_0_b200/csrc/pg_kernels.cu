@@ -102,6 +102,7 @@ __device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, int n, bool store
     rad_cyl = T.radc[rk];
     c.azi = T.yc[j0];
     c.pol = THREED ? T.zc[k + NPAD] : 0.0;
+    c.sinpol = THREED ? sin(c.pol) : 0.0;
     c.dvol0 = T.rxvol[row];
     c.vrot = T.res_v[rk] / rad_cyl;
     S.xa0[n] = T.rx[row];
@@ -115,7 +116,7 @@ __device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, int n, bool store
     bool ghost = (row < NPAD) || (row >= T.nr + NPAD);
     S.p[n] = ghost ? T.gp[rk] : (P.p0 ? P.p0[idx] : r * T.cs2[rk]);
   } else {
-    c.rad = 1.0; c.azi = 0.0; c.pol = 0.0; c.dvol0 = 1.0; c.vrot = 0.0;
+    c.rad = 1.0; c.azi = 0.0; c.pol = 0.0; c.dvol0 = 1.0; c.vrot = 0.0; c.sinpol = 0.0;
   }
   __syncthreads();
   ppm_chunk<0, SPH, THREED>(S, n, lim, st.dt, st.frrot, c, st.pl, ph);
@@ -132,17 +133,19 @@ __device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, int n, bool store
     __syncthreads();
     if (n >= NPAD && n < lim - NPAD) {
       double d1, d2, dn;
-      derivs(dn, d2, n, S.xa0, S.dx0);
-      derivs(d1, d2, n, S.xa0, S.u);
-      double t = 2.0 * nr * d2 + 2.0 * dn * d1 + 2.0 * nr * d1 / R - 2.0 * nr * S.u[n] / R / R;
-      ddu = S.u[n] + st.dt * t / rho;
-      derivs(d1, d2, n, S.xa0, S.v);
+      const DerivGeom g = deriv_geom(n, S.xa0);
+      const double iR = 1.0 / R, dtr = st.dt / rho;
+      derivs_g(dn, d2, n, g, S.dx0);
+      derivs_g(d1, d2, n, g, S.u);
+      double t = 2.0 * nr * d2 + 2.0 * dn * d1 + 2.0 * nr * d1 * iR - 2.0 * nr * S.u[n] * iR * iR;
+      ddu = S.u[n] + t * dtr;
+      derivs_g(d1, d2, n, g, S.v);
       t = R * nr * d2 + R * dn * d1 + 3.0 * nr * d1;
-      ddv = S.v[n] * R + st.dt * t / rho;
+      ddv = S.v[n] * R + t * dtr;
       if (THREED) {
-        derivs(d1, d2, n, S.xa0, S.w);
-        t = nr * d2 + dn * d1 + nr * d1 / R;
-        ddw = S.w[n] + st.dt * t / rho;
+        derivs_g(d1, d2, n, g, S.w);
+        t = nr * d2 + dn * d1 + nr * d1 * iR;
+        ddw = S.w[n] + t * dtr;
       }
     }
     __syncthreads();
@@ -258,6 +261,7 @@ __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, cons
     CellIn c;
     c.rad = rad_cyl;
     c.pol = THREED ? T.zc[k + NPAD] : 0.0;
+    c.sinpol = THREED ? sin(c.pol) : 0.0;
     c.vrot = T.res_v[rk] / rad_cyl;
     c.azi = 0.0; c.dvol0 = 1.0;
     if (act) {
@@ -295,19 +299,21 @@ __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, cons
       __syncthreads();
       if (n >= NPAD && n < lim - NPAD) {
         double d1, d2, dn;
-        derivs(dn, d2, n, S.xa0, S.dx0);
-        derivs(d1, d2, n, S.xa0, S.u);
+        const DerivGeom g = deriv_geom(n, S.xa0);
+        const double dtr = st.dt / rho;
+        derivs_g(dn, d2, n, g, S.dx0);
+        derivs_g(d1, d2, n, g, S.u);
         double t = 2.0 * nr * d2 + 2.0 * dn * d1;
         double tu = 0.0;
-        ddv = S.u[n] + st.dt * t / rho;
+        ddv = S.u[n] + t * dtr;
         if (THREED) {
-          derivs(d1, d2, n, S.xa0, S.v);
+          derivs_g(d1, d2, n, g, S.v);
           t = nr * d2 + dn * d1;
-          ddw = S.v[n] + st.dt * t / rho;
+          ddw = S.v[n] + t * dtr;
         }
-        derivs(d1, d2, n, S.xa0, S.w);
+        derivs_g(d1, d2, n, g, S.w);
         tu += nr * d2 + dn * d1;
-        ddu = S.w[n] + st.dt * tu / rho;
+        ddu = S.w[n] + tu * dtr;
       }
       __syncthreads();
       if (n >= NPAD && n < lim - NPAD) {
@@ -378,7 +384,7 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
   CellIn c;
   c.rad = rad;
   c.azi = T.yc[j0];
-  c.pol = 0.0; c.vrot = 0.0; c.dvol0 = 1.0;
+  c.pol = 0.0; c.vrot = 0.0; c.dvol0 = 1.0; c.sinpol = 0.0;
   double rad_cyl = 1.0;
   size_t idx = 0;
   if (act) {
@@ -441,11 +447,13 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
     __syncthreads();
     if (n >= NPAD && n < lim - NPAD) {
       double d1, d2, dn;
-      derivs(dn, d2, n, S.xa0, S.dx0);
-      derivs(d1, d2, n, S.xa0, S.u);
-      ddu = S.u[n] + st.dt * (2.0 * nr * d2 + 2.0 * dn * d1) / rho;
-      derivs(d1, d2, n, S.xa0, S.v);
-      ddv = S.v[n] + st.dt * (nr * d2 + dn * d1) / rho;
+      const DerivGeom g = deriv_geom(n, S.xa0);
+      const double dtr = st.dt / rho;
+      derivs_g(dn, d2, n, g, S.dx0);
+      derivs_g(d1, d2, n, g, S.u);
+      ddu = S.u[n] + (2.0 * nr * d2 + 2.0 * dn * d1) * dtr;
+      derivs_g(d1, d2, n, g, S.v);
+      ddv = S.v[n] + (nr * d2 + dn * d1) * dtr;
     }
     __syncthreads();
     if (n >= NPAD && n < lim - NPAD) { S.u[n] = ddu; S.v[n] = ddv; }

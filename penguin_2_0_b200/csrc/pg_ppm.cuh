@@ -98,6 +98,28 @@ __device__ __forceinline__ double grav_azi_sph(double rad, double azi, double po
   Rp = sqrt(Rp + p.rs * p.rs);
   return -plm * plx * sinfac / (Rp * Rp * Rp) + plm * sinpol * sinfac / plx / plx;
 }
+// the same two forces with sin(pol) formed by the caller (once per cell when
+// pol is the cell's fixed polar angle): identical arithmetic otherwise
+__device__ __forceinline__ double grav_rad_sph_s(double rad, double azi, double sinpol, const Body &p, double dt) {
+  double cosfac = cos(azi - (p.y + dt * p.vy));
+  double stm = 1.0 / (1.0 + p.m);
+  double plm = p.m * stm;
+  double plx = p.x;
+  double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac * sinpol;
+  Rp = sqrt(Rp + p.rs * p.rs);
+  return -plm * (rad - plx * cosfac * sinpol) / (Rp * Rp * Rp) - stm / (rad * rad) - plm * sinpol * cosfac / (plx * plx);
+}
+__device__ __forceinline__ double grav_azi_sph_s(double rad, double azi, double sinpol, const Body &p, double dt) {
+  double cosfac = cos(azi - (p.y + dt * p.vy));
+  double sinfac = sin(azi - (p.y + dt * p.vy));
+  rad /= sinpol;
+  double stm = 1.0 / (1.0 + p.m);
+  double plm = p.m * stm;
+  double plx = p.x;
+  double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac * sinpol;
+  Rp = sqrt(Rp + p.rs * p.rs);
+  return -plm * plx * sinfac / (Rp * Rp * Rp) + plm * sinpol * sinfac / plx / plx;
+}
 __device__ __forceinline__ double grav_pol_sph(double rad, double azi, double pol, const Body &p, double dt) {
   double cosfac = cos(azi - (p.y + dt * p.vy));
   double cospol = cos(pol);
@@ -197,6 +219,29 @@ __device__ __forceinline__ void derivs(double &first, double &second, int n, con
   double B = (x3 * h2 - x2 * h3) / (x3 - x2);
   second = 2.0 * A;
   first = second * x2 + B;
+}
+
+// derivs for several fields of one cell: the face spacings and the three
+// divisors depend on the grid only, so they are formed once per cell and the
+// divisions become products (within an ulp of derivs)
+struct DerivGeom { double x2, x3, i2, i3, i32; };
+__device__ __forceinline__ DerivGeom deriv_geom(int n, const double *xf) {
+  DerivGeom g;
+  g.x2 = xf[n] - xf[n - 1];
+  g.x3 = xf[n + 1] - xf[n - 1];
+  g.i2 = 1.0 / g.x2;
+  g.i3 = 1.0 / g.x3;
+  g.i32 = 1.0 / (g.x3 - g.x2);
+  return g;
+}
+__device__ __forceinline__ void derivs_g(double &first, double &second, int n, const DerivGeom &g,
+                                         const double *u) {
+  double h2 = (u[n] - u[n - 1]) * g.i2;
+  double h3 = (u[n + 1] - u[n - 1]) * g.i3;
+  double A = (h3 - h2) * g.i32;
+  double B = (g.x3 * h2 - g.x2 * h3) * g.i32;
+  second = 2.0 * A;
+  first = second * g.x2 + B;
 }
 
 }  // namespace pgd

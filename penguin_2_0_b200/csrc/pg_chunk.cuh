@@ -53,10 +53,11 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
     // get_fz_bound forces.cu:298-334 (ngeomz 5) at the face angle xa0[n]
     double pol = S.xa0[n];
     double azi = c.azi + hdt * c.vrot;
-    double grav = ph.plnt ? grav_pol_sph(c.rad, azi, pol, pl, hdt) : 0.0;
-    double rad_cyl = c.rad * sin(pol);
+    const double sp = sin(pol), cp = cos(pol);
+    double grav = ph.plnt ? grav_pol_sph_s(c.rad, azi, sp, cp, pl, hdt) : 0.0;
+    double rad_cyl = c.rad * sp;
     double f = grav;
-    f += (sq(0.5 * (S.w[n] + S.w[n - 1])) * cos(pol)) / rad_cyl / rad_cyl / rad_cyl;
+    f += (sq(0.5 * (S.w[n] + S.w[n - 1])) * cp) / rad_cyl / rad_cyl / rad_cyl;
     ftot = f;
   }
 }
@@ -84,10 +85,11 @@ __device__ __forceinline__ double centre_force(int n, double dt, double rad, dou
     if (!SPH) return ph.plnt ? grav_azi_cyl(rad, azi, pol, pl, dt) : 0.0;
     return ph.plnt ? grav_azi_sph_s(rad, azi, sinpol, pl, dt) : 0.0;
   } else {
-    double grav = ph.plnt ? grav_pol_sph(rad, azi, pol, pl, dt) : 0.0;
-    double rad_cyl = rad * sin(pol);
+    const double sp = sin(pol), cp = cos(pol);
+    double grav = ph.plnt ? grav_pol_sph_s(rad, azi, sp, cp, pl, dt) : 0.0;
+    double rad_cyl = rad * sp;
     double f = grav;
-    f += (S.w[n] * S.w[n] * cos(pol)) / rad_cyl / rad_cyl / rad_cyl;
+    f += (S.w[n] * S.w[n] * cp) / rad_cyl / rad_cyl / rad_cyl;
     return f;
   }
 }

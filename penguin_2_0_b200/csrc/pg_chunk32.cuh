@@ -49,6 +49,7 @@ struct CellIn32 {
   double omres;   // azimuthal sweep: v_bg / r_cyl - v_rot - FrRot (FP64)
   double sig;     // this cell's Sigma in FP64 (S_bg + dS)
   double dx0;     // this cell's Eulerian width in FP64
+  double sinpol;  // sin(pol) for the radial and azimuthal sweeps in 3D
 };
 
 __device__ __forceinline__ float min3f(float A, float B, float C) {
@@ -150,30 +151,31 @@ __device__ __forceinline__ double face_force32(int n, double hdt, const CellIn32
       double vf = 0.5 * (Lv[n] + Lv[n - 1]);
       return grav + vf * vf / rad / rad / rad;
     } else {
-      grav = ph.plnt ? grav_rad_sph(rad, azi, c.pol, pl, hdt) : -1.0 / rad / rad;
+      grav = ph.plnt ? grav_rad_sph_s(rad, azi, c.sinpol, pl, hdt) : -1.0 / rad / rad;
       double wf = 0.5 * ((double)wv[n] + (double)wv[n - 1]);
       double vf = 0.5 * (Lv[n] + Lv[n - 1]);
-      double rs = rad * sin(c.pol);
+      double rs = rad * c.sinpol;
       return grav + wf * wf / rad / rad / rad + vf * vf / rad / (rs * rs);
     }
   } else if (AXIS == 1) {
     double azi = xa0f + hdt * c.vrot;
     if (!SPH) return ph.plnt ? grav_azi_cyl(c.rad, azi, c.pol, pl, hdt) : 0.0;
-    return ph.plnt ? grav_azi_sph(c.rad, azi, c.pol, pl, hdt) : 0.0;
+    return ph.plnt ? grav_azi_sph_s(c.rad, azi, c.sinpol, pl, hdt) : 0.0;
   } else {
     double pol = xa0f;
     double azi = c.azi + hdt * c.vrot;
-    double grav = ph.plnt ? grav_pol_sph(c.rad, azi, pol, pl, hdt) : 0.0;
-    double rc = c.rad * sin(pol);
+    const double sp = sin(pol), cp = cos(pol);
+    double grav = ph.plnt ? grav_pol_sph_s(c.rad, azi, sp, cp, pl, hdt) : 0.0;
+    double rc = c.rad * sp;
     double lf = 0.5 * (Lv[n] + Lv[n - 1]);
-    return grav + (lf * lf * cos(pol)) / rc / rc / rc;
+    return grav + (lf * lf * cp) / rc / rc / rc;
   }
 }
 
 template <int AXIS, bool SPH>
 __device__ __forceinline__ double centre_force32(int n, double dt, double rad, double azi, double pol,
-                                                 const double *Lv, const float *wv, const Body &pl,
-                                                 const Phys &ph) {
+                                                 double sinpol, const double *Lv, const float *wv,
+                                                 const Body &pl, const Phys &ph) {
   if (AXIS == 0) {
     double grav;
     if (!SPH) {
@@ -181,18 +183,19 @@ __device__ __forceinline__ double centre_force32(int n, double dt, double rad, d
       else { double dis = sqrt(rad * rad + pol * pol); grav = -rad / dis / dis / dis; }
       return grav + Lv[n] * Lv[n] / rad / rad / rad;
     } else {
-      grav = ph.plnt ? grav_rad_sph(rad, azi, pol, pl, dt) : -1.0 / rad / rad;
+      grav = ph.plnt ? grav_rad_sph_s(rad, azi, sinpol, pl, dt) : -1.0 / rad / rad;
       double w = wv[n];
-      double rs = rad * sin(pol);
+      double rs = rad * sinpol;
       return grav + w * w / rad / rad / rad + Lv[n] * Lv[n] / rad / (rs * rs);
     }
   } else if (AXIS == 1) {
     if (!SPH) return ph.plnt ? grav_azi_cyl(rad, azi, pol, pl, dt) : 0.0;
-    return ph.plnt ? grav_azi_sph(rad, azi, pol, pl, dt) : 0.0;
+    return ph.plnt ? grav_azi_sph_s(rad, azi, sinpol, pl, dt) : 0.0;
   } else {
-    double grav = ph.plnt ? grav_pol_sph(rad, azi, pol, pl, dt) : 0.0;
-    double rc = rad * sin(pol);
-    return grav + (Lv[n] * Lv[n] * cos(pol)) / rc / rc / rc;
+    const double sp = sin(pol), cp = cos(pol);
+    double grav = ph.plnt ? grav_pol_sph_s(rad, azi, sp, cp, pl, dt) : 0.0;
+    double rc = rad * sp;
+    return grav + (Lv[n] * Lv[n] * cp) / rc / rc / rc;
   }
 }
 
@@ -311,14 +314,14 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
     double xcl = xa + 0.5 * dxld;
     double a1, a2;
     if (AXIS == 0) {
-      a1 = centre_force32<0, SPH>(n, 0.0, c.rad, c.azi, c.pol, S.L, S.w, pl, ph);
-      a2 = centre_force32<0, SPH>(n, dt, xcl, c.azi + dt * c.vrot, c.pol, S.L, S.w, pl, ph);
+      a1 = centre_force32<0, SPH>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S.L, S.w, pl, ph);
+      a2 = centre_force32<0, SPH>(n, dt, xcl, c.azi + dt * c.vrot, c.pol, c.sinpol, S.L, S.w, pl, ph);
     } else if (AXIS == 1) {
-      a1 = centre_force32<1, SPH>(n, 0.0, c.rad, c.azi, c.pol, S.L, S.v, pl, ph);
-      a2 = centre_force32<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, S.L, S.v, pl, ph);
+      a1 = centre_force32<1, SPH>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S.L, S.v, pl, ph);
+      a2 = centre_force32<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, c.sinpol, S.L, S.v, pl, ph);
     } else {
-      a1 = centre_force32<2, SPH>(n, 0.0, c.rad, c.azi, c.pol, S.L, S.v, pl, ph);
-      a2 = centre_force32<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, S.L, S.v, pl, ph);
+      a1 = centre_force32<2, SPH>(n, 0.0, c.rad, c.azi, c.pol, 0.0, S.L, S.v, pl, ph);
+      a2 = centre_force32<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, 0.0, S.L, S.v, pl, ph);
     }
     fto1 = (float)a1;
     fto2 = (float)a2;

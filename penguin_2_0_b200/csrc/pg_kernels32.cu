@@ -57,15 +57,25 @@ __device__ __forceinline__ bool load_step32(const SweepCtl &c, StepIn32 &s) {
 // three-point derivatives of derivs (viscosity.cu:2-18) written with cell
 // widths: xf[n]-xf[n-1] = w[n-1], xf[n+1]-xf[n-1] = w[n-1] + w[n]
 template <typename T>
-__device__ __forceinline__ void derivs_w(T &first, T &second, int n, const float *w, T scale, const T *u) {
-  T x2 = (T)w[n - 1] * scale;
-  T x3 = x2 + (T)w[n] * scale;
-  T h2 = (u[n] - u[n - 1]) / x2;
-  T h3 = (u[n + 1] - u[n - 1]) / x3;
-  T A = (h3 - h2) / (x3 - x2);
-  T B = (x3 * h2 - x2 * h3) / (x3 - x2);
+struct DerivGeomW { T x2, x3, i2, i3, i32; };
+template <typename T>
+__device__ __forceinline__ DerivGeomW<T> deriv_geom_w(int n, const float *w, T scale) {
+  DerivGeomW<T> g;
+  g.x2 = (T)w[n - 1] * scale;
+  g.x3 = g.x2 + (T)w[n] * scale;
+  g.i2 = (T)1 / g.x2;
+  g.i3 = (T)1 / g.x3;
+  g.i32 = (T)1 / (g.x3 - g.x2);
+  return g;
+}
+template <typename T>
+__device__ __forceinline__ void derivs_w(T &first, T &second, int n, const DerivGeomW<T> &g, const T *u) {
+  T h2 = (u[n] - u[n - 1]) * g.i2;
+  T h3 = (u[n + 1] - u[n - 1]) * g.i3;
+  T A = (h3 - h2) * g.i32;
+  T B = (g.x3 * h2 - g.x2 * h3) * g.i32;
   second = (T)2 * A;
-  first = second * x2 + B;
+  first = second * g.x2 + B;
 }
 
 // ---------------------------------------------------------------------------
@@ -100,6 +110,7 @@ __device__ __forceinline__ void sweep_x32_body(ChunkShm32<NT> &S, int n, bool st
     sbg = T.sbg[rk];
     c.azi = T.yc[j0];
     c.pol = THREED ? T.zc[k + NPAD] : 0.0;
+    c.sinpol = THREED ? sin(c.pol) : 0.0;
     c.dvol0 = T.rxvol[row];
     c.vrot = T.res_v[rk] / rad_cyl;
     S.xa0[n] = T.rx[row];
@@ -133,17 +144,19 @@ __device__ __forceinline__ void sweep_x32_body(ChunkShm32<NT> &S, int n, bool st
     __syncthreads();
     if (n >= NPAD && n < lim - NPAD) {
       float d1, d2, dn;
+      const DerivGeomW<float> gf = deriv_geom_w<float>(n, S.dx0, 1.0f);
+      const DerivGeomW<double> gd = deriv_geom_w<double>(n, S.dx0, 1.0);
       const float Rf = (float)R;
-      derivs_w<float>(dn, d2, n, S.dx0, 1.0f, nn);
-      derivs_w<float>(d1, d2, n, S.dx0, 1.0f, S.u);
+      derivs_w<float>(dn, d2, n, gf, nn);
+      derivs_w<float>(d1, d2, n, gf, S.u);
       float t = 2.0f * nr * d2 + 2.0f * dn * d1 + 2.0f * nr * d1 / Rf - 2.0f * nr * S.u[n] / Rf / Rf;
       ddu = S.u[n] + (float)st.dt * t / rho;
       double e1, e2;
-      derivs_w<double>(e1, e2, n, S.dx0, 1.0, om);
+      derivs_w<double>(e1, e2, n, gd, om);
       double tv = R * (double)nr * e2 + R * (double)dn * e1 + 3.0 * (double)nr * e1;
       ddv = om[n] * R + st.dt * tv / (double)rho;
       if (THREED) {
-        derivs_w<float>(d1, d2, n, S.dx0, 1.0f, S.w);
+        derivs_w<float>(d1, d2, n, gf, S.w);
         t = nr * d2 + dn * d1 + nr * d1 / Rf;
         ddw = S.w[n] + (float)st.dt * t / rho;
       }
@@ -263,9 +276,10 @@ __device__ __forceinline__ void sweep_y32_body(ChunkShm32<NT> &S, double *red, c
     CellIn32 c;
     c.rad = rad_cyl;
     c.pol = THREED ? T.zc[k + NPAD] : 0.0;
+    c.sinpol = THREED ? sin(c.pol) : 0.0;
     c.vrot = T.res_v[rk] / rad_cyl;
     c.omres = vbg / rad_cyl - c.vrot - st.frrot;
-    c.azi = 0.0; c.dvol0 = 1.0; c.sig = 1.0;
+    c.azi = 0.0; c.dvol0 = 1.0; c.sig = 1.0; c.dx0 = 0.0;
     if (act) {
       size_t s = base + j0;
       double azi = T.yc[j0];
@@ -302,17 +316,18 @@ __device__ __forceinline__ void sweep_y32_body(ChunkShm32<NT> &S, double *red, c
       __syncthreads();
       if (n >= NPAD && n < lim - NPAD) {
         float d1, d2, dn;
-        derivs_w<float>(dn, d2, n, S.dx0, R, nn);
-        derivs_w<float>(d1, d2, n, S.dx0, R, S.u);
+        const DerivGeomW<float> gf = deriv_geom_w<float>(n, S.dx0, R);
+        derivs_w<float>(dn, d2, n, gf, nn);
+        derivs_w<float>(d1, d2, n, gf, S.u);
         float t = 2.0f * nr * d2 + 2.0f * dn * d1;
         float tu = 0.0f;
         ddv = S.u[n] + (float)st.dt * t / rho;
         if (THREED) {
-          derivs_w<float>(d1, d2, n, S.dx0, R, S.v);
+          derivs_w<float>(d1, d2, n, gf, S.v);
           t = nr * d2 + dn * d1;
           ddw = S.v[n] + (float)st.dt * t / rho;
         }
-        derivs_w<float>(d1, d2, n, S.dx0, R, S.w);
+        derivs_w<float>(d1, d2, n, gf, S.w);
         tu += nr * d2 + dn * d1;
         ddu = S.w[n] + (float)st.dt * tu / rho;
       }
@@ -436,10 +451,11 @@ __device__ __forceinline__ void sweep_z32_body(ChunkShm32<NT> &S, int n, bool st
     __syncthreads();
     if (n >= NPAD && n < lim - NPAD) {
       float d1, d2, dn;
-      derivs_w<float>(dn, d2, n, S.dx0, R, nn);
-      derivs_w<float>(d1, d2, n, S.dx0, R, S.u);
+      const DerivGeomW<float> gf = deriv_geom_w<float>(n, S.dx0, R);
+      derivs_w<float>(dn, d2, n, gf, nn);
+      derivs_w<float>(d1, d2, n, gf, S.u);
       ddu = S.u[n] + (float)st.dt * (2.0f * nr * d2 + 2.0f * dn * d1) / rho;
-      derivs_w<float>(d1, d2, n, S.dx0, R, S.v);
+      derivs_w<float>(d1, d2, n, gf, S.v);
       ddv = S.v[n] + (float)st.dt * (nr * d2 + dn * d1) / rho;
     }
     __syncthreads();

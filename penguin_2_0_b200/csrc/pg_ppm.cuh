@@ -120,6 +120,17 @@ __device__ __forceinline__ double grav_azi_sph_s(double rad, double azi, double 
   Rp = sqrt(Rp + p.rs * p.rs);
   return -plm * plx * sinfac / (Rp * Rp * Rp) + plm * sinpol * sinfac / plx / plx;
 }
+__device__ __forceinline__ double grav_pol_sph_s(double rad, double azi, double sinpol, double cospol,
+                                                 const Body &p, double dt) {
+  double cosfac = cos(azi - (p.y + dt * p.vy));
+  double stm = 1.0 / (1.0 + p.m);
+  double plm = p.m * stm;
+  double plx = p.x;
+  (void)stm;
+  double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac * sinpol;
+  Rp = sqrt(Rp + p.rs * p.rs);
+  return plm * plx * cosfac * cospol / (Rp * Rp * Rp) - plm * cosfac * cospol / (sinpol * plx * plx);
+}
 __device__ __forceinline__ double grav_pol_sph(double rad, double azi, double pol, const Body &p, double dt) {
   double cosfac = cos(azi - (p.y + dt * p.vy));
   double cospol = cos(pol);

@@ -30,18 +30,21 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
     // get_fx_bound forces.cu:185-224 at the left face xa0[n]
     double rad = S.xa0[n];
     double azi = c.azi + hdt * c.vrot;
+    // x / r / r / r of forces.cu as x r^-3; products rounded on their own
+    // (no fused multiply-add) so that every kernel shape gives the same bits
+    const double ir = 1.0 / rad, ir2 = __dmul_rn(ir, ir), ir3 = __dmul_rn(ir2, ir);
     double grav;
     if (!SPH) {
-      if (ph.plnt) { grav = grav_rad_cyl(rad, azi, c.pol, pl, hdt); grav += -1.0 / rad / rad; }
+      if (ph.plnt) { grav = grav_rad_cyl(rad, azi, c.pol, pl, hdt); grav += -ir2; }
       else { double dis = sqrt(rad * rad + c.pol * c.pol); grav = -rad / dis / dis / dis; }
       double f = grav;
-      f += sq(0.5 * (S.v[n] + S.v[n - 1])) / rad / rad / rad;
+      f += __dmul_rn(sq(0.5 * (S.v[n] + S.v[n - 1])), ir3);
       ftot = f;
     } else {
-      grav = ph.plnt ? grav_rad_sph_s(rad, azi, c.sinpol, pl, hdt) : -1.0 / rad / rad;
+      grav = ph.plnt ? grav_rad_sph_s(rad, azi, c.sinpol, pl, hdt) : -ir2;
       double f = grav;
-      f += sq(0.5 * (S.w[n] + S.w[n - 1])) / rad / rad / rad;
-      f += sq(0.5 * (S.v[n] + S.v[n - 1])) / rad / sq(rad * c.sinpol);
+      f += __dmul_rn(sq(0.5 * (S.w[n] + S.w[n - 1])), ir3);
+      f += __dmul_rn(sq(0.5 * (S.v[n] + S.v[n - 1])), ir) / sq(rad * c.sinpol);
       ftot = f;
     }
   } else if (AXIS == 1) {
@@ -55,9 +58,9 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
     double azi = c.azi + hdt * c.vrot;
     const double sp = sin(pol), cp = cos(pol);
     double grav = ph.plnt ? grav_pol_sph_s(c.rad, azi, sp, cp, pl, hdt) : 0.0;
-    double rad_cyl = c.rad * sp;
+    double irc = 1.0 / (c.rad * sp);
     double f = grav;
-    f += (sq(0.5 * (S.w[n] + S.w[n - 1])) * cp) / rad_cyl / rad_cyl / rad_cyl;
+    f += __dmul_rn(sq(0.5 * (S.w[n] + S.w[n - 1])) * cp, __dmul_rn(__dmul_rn(irc, irc), irc));
     ftot = f;
   }
 }
@@ -68,17 +71,18 @@ __device__ __forceinline__ double centre_force(int n, double dt, double rad, dou
                                                double sinpol, const SHM &S, const Body &pl, const Phys &ph) {
   if (AXIS == 0) {
     double grav;
+    const double ir = 1.0 / rad, ir2 = __dmul_rn(ir, ir), ir3 = __dmul_rn(ir2, ir);
     if (!SPH) {
-      if (ph.plnt) { grav = grav_rad_cyl(rad, azi, pol, pl, dt); grav += -1.0 / rad / rad; }
+      if (ph.plnt) { grav = grav_rad_cyl(rad, azi, pol, pl, dt); grav += -ir2; }
       else { double dis = sqrt(rad * rad + pol * pol); grav = -rad / dis / dis / dis; }
       double f = grav;
-      f += S.v[n] * S.v[n] / rad / rad / rad;
+      f += __dmul_rn(__dmul_rn(S.v[n], S.v[n]), ir3);
       return f;
     } else {
-      grav = ph.plnt ? grav_rad_sph_s(rad, azi, sinpol, pl, dt) : -1.0 / rad / rad;
+      grav = ph.plnt ? grav_rad_sph_s(rad, azi, sinpol, pl, dt) : -ir2;
       double f = grav;
-      f += S.w[n] * S.w[n] / rad / rad / rad;
-      f += S.v[n] * S.v[n] / rad / sq(rad * sinpol);
+      f += __dmul_rn(__dmul_rn(S.w[n], S.w[n]), ir3);
+      f += __dmul_rn(__dmul_rn(S.v[n], S.v[n]), ir) / sq(rad * sinpol);
       return f;
     }
   } else if (AXIS == 1) {
@@ -87,9 +91,9 @@ __device__ __forceinline__ double centre_force(int n, double dt, double rad, dou
   } else {
     const double sp = sin(pol), cp = cos(pol);
     double grav = ph.plnt ? grav_pol_sph_s(rad, azi, sp, cp, pl, dt) : 0.0;
-    double rad_cyl = rad * sp;
+    double irc = 1.0 / (rad * sp);
     double f = grav;
-    f += (S.w[n] * S.w[n] * cp) / rad_cyl / rad_cyl / rad_cyl;
+    f += __dmul_rn(S.w[n] * S.w[n] * cp, __dmul_rn(__dmul_rn(irc, irc), irc));
     return f;
   }
 }

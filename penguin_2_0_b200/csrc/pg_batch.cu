@@ -42,9 +42,9 @@ __global__ void kb_status(pgd::DevClock *const *clks, int n, pg_batch_member *ou
 struct Group {
   std::vector<pg_run *> members;
   pgd::BatchRun *d_runs = nullptr;
-  int *d_start = nullptr;          // [3][n+1]: radial tiles, azimuthal tiles, rings
+  int *d_start = nullptr;          // [4][n+1]: radial tiles, azimuthal tiles, rings, short radial tiles
   size_t cap = 0;
-  pgd::BatchQueue qx{}, qy{}, qr{};
+  pgd::BatchQueue qx{}, qy{}, qr{}, qxs{};
   pg_batch_shape shape{0, 0, 8, 0};
 };
 
@@ -112,11 +112,11 @@ static int rebuild(pg_batch *b) {
       g.d_start = nullptr;
       size_t cap = std::max<size_t>(n, 16);
       BK(cudaMalloc(&g.d_runs, cap * sizeof(pgd::BatchRun)));
-      BK(cudaMalloc(&g.d_start, 3 * (cap + 1) * sizeof(int)));
+      BK(cudaMalloc(&g.d_start, 4 * (cap + 1) * sizeof(int)));
       g.cap = cap;
     }
     std::vector<pgd::BatchRun> h(n);
-    std::vector<int> st(3 * (n + 1), 0);
+    std::vector<int> st(4 * (n + 1), 0);
     for (size_t i = 0; i < n; i++) {
       pg_run *r = g.members[i];
       if (int e = pgi::run_batch_desc(r, &h[i])) return bfail(b, e, pg_last_error(r));
@@ -125,6 +125,7 @@ static int rebuild(pg_batch *b) {
       st[i + 1] = st[i] + sh.tiles_x;
       st[(n + 1) + i + 1] = st[(n + 1) + i] + sh.tiles_y;
       st[2 * (n + 1) + i + 1] = st[2 * (n + 1) + i] + sh.nr;
+      st[3 * (n + 1) + i + 1] = st[3 * (n + 1) + i] + sh.tiles_xs;
     }
     if (n) {
       BK(cudaMemcpy(g.d_runs, h.data(), n * sizeof(pgd::BatchRun), cudaMemcpyHostToDevice));
@@ -134,6 +135,7 @@ static int rebuild(pg_batch *b) {
     g.qx = {g.d_runs, g.d_start, ni, st[n]};
     g.qy = {g.d_runs, g.d_start + (n + 1), ni, st[(n + 1) + n]};
     g.qr = {g.d_runs, g.d_start + 2 * (n + 1), ni, st[2 * (n + 1) + n]};
+    g.qxs = {g.d_runs, g.d_start + 3 * (n + 1), ni, st[3 * (n + 1) + n]};
   }
   size_t n = b->runs.size();
   if (n > b->status_cap) {
@@ -163,16 +165,18 @@ static void enqueue_group_step(pg_batch *b, int gi, int64_t *nk) {
   pgk::batch_prestep(g.d_runs, n, s);
   if (gi == 1) {
     pgk::batch_sweep_x32(g.qx, g.shape.grid_x, g.shape.minb, s);
+    pgk::batch_sweep_x32_short(g.qxs, s);
     pgk::batch_sweep_y32(g.qy, g.shape.grid_y, g.shape.minb, s);
   } else {
     pgk::batch_sweep_x(g.qx, g.shape.grid_x, g.shape.minb, s);
+    pgk::batch_sweep_x_short(g.qxs, s);
     pgk::batch_sweep_y(g.qy, g.shape.grid_y, g.shape.minb, s);
   }
   pgk::batch_poststep(g.d_runs, n, s);
   pgk::batch_reduce(g.qr, gi, 0, s);
   pgk::batch_reduce(g.qr, gi, 9, s);
   pgk::batch_record(g.d_runs, n, s);
-  *nk += 8;
+  *nk += 8 + (g.qxs.total > 0 ? 1 : 0);
 }
 
 // one step of every member, on the batch stream

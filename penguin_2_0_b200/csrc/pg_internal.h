@@ -13,6 +13,8 @@ struct RunShape {
   int dev, ndim, fp32, loaded, clock_ready, p0_live;
   int nr, nphi, nk;
   int tiles_x, tiles_y;    // 2D pencil chunks of the radial and azimuthal sweeps
+  int tiles_xs;            // radial last chunks of at most 64 cells, 4 columns per tile
+                           // (then not counted in tiles_x)
 };
 int run_shape(const pg_run *run, RunShape *out);
 

@@ -991,6 +991,30 @@ __global__ void __launch_bounds__(128, MINB) kb_sweep_x(BatchQueue q) {
   }
 }
 
+// radial last chunks of at most 64 cells: tile t of a member covers columns
+// 4t .. 4t+3, thread i on cell i / 4 of column 4t + i % 4 (threads past the
+// chunk's lim idle; columns past the last one repeat it without storing)
+__global__ void __launch_bounds__(256, 4) kb_sweep_x_short(BatchQueue q) {
+  __shared__ ChunkShmT<64> S[4];
+  for (int t = blockIdx.x; t < q.total; t += gridDim.x) {
+    const int r = batch_find(q, t);
+    const BatchRun &b = q.runs[r];
+    SweepCtl ctl{};
+    ctl.clk = b.clk;
+    StepIn st;
+    if (load_step(ctl, st)) {
+      const int p = threadIdx.x & 3, n = threadIdx.x >> 2, nphi = b.T.nphi;
+      int col = 4 * (t - q.start[r]) + p;
+      const bool store = col < nphi;
+      if (!store) col = nphi - 1;
+      Planes P = b.PX;
+      P.p0 = (b.p0 && b.clk->ncycle == b.p0_cycle) ? b.p0 : nullptr;
+      sweep_x_body<false, false, 64>(S[p], n, store, b.T, P, b.ph, ctl, st, col, b.T.cx.loop - 1, 0);
+    }
+    __syncthreads();
+  }
+}
+
 template <int MINB>
 __global__ void __launch_bounds__(128, MINB) kb_sweep_y(BatchQueue q) {
   __shared__ ChunkShmT<128> S;
@@ -1195,6 +1219,9 @@ void batch_sweep_x(const BatchQueue &q, int grid, int minb, cudaStream_t s) {
   int g = (grid > 0 && grid < q.total) ? grid : q.total;
   if (minb >= 8) kb_sweep_x<8><<<g, 128, 0, s>>>(q);
   else kb_sweep_x<4><<<g, 128, 0, s>>>(q);
+}
+void batch_sweep_x_short(const BatchQueue &q, cudaStream_t s) {
+  if (q.total > 0) kb_sweep_x_short<<<q.total, 256, 0, s>>>(q);
 }
 void batch_sweep_y(const BatchQueue &q, int grid, int minb, cudaStream_t s) {
   if (q.total <= 0) return;

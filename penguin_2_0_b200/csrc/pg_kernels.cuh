@@ -143,6 +143,8 @@ void batch_poststep(const BatchRun *runs, int nruns, cudaStream_t s);
 void batch_record(const BatchRun *runs, int nruns, cudaStream_t s);
 void batch_reduce(const BatchQueue &rings, int fp32, int mode, cudaStream_t s);
 void batch_sweep_x(const BatchQueue &q, int grid, int minb, cudaStream_t s);
+void batch_sweep_x_short(const BatchQueue &q, cudaStream_t s);
+void batch_sweep_x32_short(const BatchQueue &q, cudaStream_t s);
 void batch_sweep_y(const BatchQueue &q, int grid, int minb, cudaStream_t s);
 void batch_sweep_x32(const BatchQueue &q, int grid, int minb, cudaStream_t s);
 void batch_sweep_y32(const BatchQueue &q, int grid, int minb, cudaStream_t s);

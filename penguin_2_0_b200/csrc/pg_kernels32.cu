@@ -596,6 +596,26 @@ __global__ void __launch_bounds__(128, MINB) kb32_sweep_x(BatchQueue q) {
   }
 }
 
+// radial last chunks of at most 64 cells, 4 columns per tile (see kb_sweep_x_short)
+__global__ void __launch_bounds__(256, 4) kb32_sweep_x_short(BatchQueue q) {
+  __shared__ ChunkShm32<64> S[4];
+  for (int t = blockIdx.x; t < q.total; t += gridDim.x) {
+    const int r = batch_find32(q, t);
+    const BatchRun &b = q.runs[r];
+    SweepCtl ctl{};
+    ctl.clk = b.clk;
+    StepIn32 st;
+    if (load_step32(ctl, st)) {
+      const int p = threadIdx.x & 3, n = threadIdx.x >> 2, nphi = b.T.nphi;
+      int col = 4 * (t - q.start[r]) + p;
+      const bool store = col < nphi;
+      if (!store) col = nphi - 1;
+      sweep_x32_body<false, false, 64>(S[p], n, store, b.T, b.QX, b.ph, ctl, st, col, b.T.cx.loop - 1, 0);
+    }
+    __syncthreads();
+  }
+}
+
 template <int MINB>
 __global__ void __launch_bounds__(128, MINB) kb32_sweep_y(BatchQueue q) {
   __shared__ ChunkShm32<128> S;
@@ -717,6 +737,9 @@ void batch_sweep_x32(const BatchQueue &q, int grid, int minb, cudaStream_t s) {
   int g = (grid > 0 && grid < q.total) ? grid : q.total;
   if (minb >= 8) kb32_sweep_x<8><<<g, 128, 0, s>>>(q);
   else kb32_sweep_x<4><<<g, 128, 0, s>>>(q);
+}
+void batch_sweep_x32_short(const BatchQueue &q, cudaStream_t s) {
+  if (q.total > 0) kb32_sweep_x_short<<<q.total, 256, 0, s>>>(q);
 }
 void batch_sweep_y32(const BatchQueue &q, int grid, int minb, cudaStream_t s) {
   if (q.total <= 0) return;

@@ -1161,7 +1161,10 @@ int run_shape(const pg_run *run, RunShape *o) {
   o->clock_ready = run->clock_ready ? 1 : 0;
   o->p0_live = run->p0_live ? 1 : 0;
   o->nr = run->nr; o->nphi = run->nphi; o->nk = run->nk;
-  o->tiles_x = run->nphi * run->T.cx.loop * run->nk;
+  const pgd::Chunking &cx = run->T.cx;
+  const bool short_last = !cx.stuck && cx.lim_last <= 64;
+  o->tiles_x = run->nphi * (cx.loop - (short_last ? 1 : 0)) * run->nk;
+  o->tiles_xs = short_last ? (run->nphi * run->nk + 3) / 4 : 0;
   o->tiles_y = run->T.cy.loop * run->nr * run->nk;
   return PG_OK;
 }

@@ -332,7 +332,7 @@ __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, cons
     double m = block_max(rate, red);
     int anybad = __syncthreads_or(bad);
     if (n == 0) {
-      if (m > 0.0 || m != m) atomicMax(&ctl.clk->cfl_bits, dbits(m));
+      if (!ctl.nocfl && (m > 0.0 || m != m)) atomicMax(&ctl.clk->cfl_bits, dbits(m));
       if (anybad) atomicExch(&ctl.clk->status, 3);
     }
   }
@@ -638,7 +638,7 @@ __global__ void k_damp_clk(Tables T, double *R, double *U, double *V, double *W,
 
 // CFL rate for the next step (3D fused loop): rot_j has not been rotated yet
 __global__ void k_cfl_clk(Tables T, const double *R, const double *U, const double *V, const double *W,
-                          Phys ph, DevClock *clk) {
+                          Phys ph, DevClock *clk, int ndim, int rot_pending) {
   __shared__ double red[32];
   if (clk->halted) return;
   int i = blockIdx.x, k = blockIdx.y;
@@ -646,7 +646,7 @@ __global__ void k_cfl_clk(Tables T, const double *R, const double *U, const doub
   size_t base = (size_t)rk * T.nphi;
   double rad = T.rxc[row], rad_cyl = T.radc[rk];
   double frrot = clk->frrot_next;
-  int rotn = T.rot_j[rk] + T.inc_j[rk];
+  int rotn = T.rot_j[rk] + (rot_pending ? T.inc_j[rk] : 0);
   double rate = 0.0;
   bool bad = false;
   for (int j = threadIdx.x; j < T.nphi; j += blockDim.x) {
@@ -656,8 +656,13 @@ __global__ void k_cfl_clk(Tables T, const double *R, const double *U, const doub
     double cs = sqrt(ph.gam * p / r);
     double t0 = (fabs(U[base + j]) + cs) / T.rdx[row];
     double t1 = (fabs(V[base + j] - T.rot_v[rk] - frrot * rad_cyl) + cs) / (T.dy[js] * rad_cyl);
-    double t2 = (fabs(W[base + j]) + cs) / (T.dz[k + NPAD] * rad);
-    double rt = max3(t0, t1, t2);
+    double rt;
+    if (ndim == 3) {
+      double t2 = (fabs(W[base + j]) + cs) / (T.dz[k + NPAD] * rad);
+      rt = max3(t0, t1, t2);
+    } else {
+      rt = fmax(t0, t1);
+    }
     rate = (rt > rate || rt != rt) ? rt : rate;
     if (!(r > 0.0) || !isfinite(r) || !isfinite(U[base + j]) || !isfinite(V[base + j])) bad = true;
   }
@@ -689,11 +694,13 @@ template <typename RT>
 __device__ __forceinline__ void reduce_body(const Tables &T, const RT *R, Body pl, const DevClock *clk,
                                             double exclude, int mode, int plnt, double p_alpha, int ndim,
                                             double *ring_part, unsigned int *counter, double *out,
-                                            double *hist_row, int i, int k, unsigned nblocks) {
+                                            double *hist_row, int i, int k, unsigned nblocks,
+                                            bool every_step = false) {
   __shared__ double list[1024];
   __shared__ bool is_last;
   if (clk) {
-    if (!clk->prin) return;
+    if (!every_step && !clk->prin) return;
+    if (every_step && clk->halted) return;
     pl = clk->planet;
   }
   const int row = i + NPAD, rk = k * T.nrg + row;
@@ -797,6 +804,16 @@ __global__ void __launch_bounds__(1024) k_reduce(Tables T, const RT *R, Body pl,
                   blockIdx.x, blockIdx.y, gridDim.x * gridDim.y);
 }
 
+// moving planet: the disk's radial (mode 8) and azimuthal (mode 9) force
+// sums on the drifted planet, every step, into the clock
+template <typename RT>
+__global__ void __launch_bounds__(1024) k_reduce_forces(Tables T, const RT *R, DevClock *clk, int mode,
+                                                        double p_alpha, int ndim, double *ring_part,
+                                                        unsigned int *counter) {
+  reduce_body<RT>(T, R, Body{}, clk, 0.0, mode, 1, p_alpha, ndim, ring_part, counter,
+                  mode == 8 ? &clk->f8 : &clk->f9, nullptr, blockIdx.x, blockIdx.y, gridDim.x * gridDim.y, true);
+}
+
 // append a diagnostics row when this step prints (main.cu:414-428)
 __device__ __forceinline__ void record_body(DevClock *clk) {
   DevClock &c = *clk;
@@ -842,6 +859,13 @@ __device__ void d_drift(Body &pl, double FrRot, double dt, const DevClock &c) {
   // rs = rs_fac*get_h(x), get_h = sqrt(cs2(x) x^3); cs2 = sc2 * x^-p_beta is
   // evaluated on the host for the fixed-orbit case and never changes there
   (void)c;
+}
+// moving planet: the drift moves x, and the softening follows it as
+// kick_drift_kick does on the host, rs = rs_fac h(x), h = sqrt(cs2(x) x^3)
+// with cs2 = sc_h^2 x^-p_beta (disk_profile.cu:39-52)
+__device__ void d_drift_moving(Body &pl, double FrRot, double dt, const DevClock &c) {
+  d_drift(pl, FrRot, dt, c);
+  pl.rs = c.rs_fac * sqrt(c.sc2 * pow(pl.x, -c.p_beta) * pl.x * pl.x * pl.x);
 }
 __device__ void d_forces_fixed(Body &pl, double FrRot) {
   pl.fx = -1.0 / pl.x / pl.x + pl.x * pow(pl.vy + FrRot, 2);
@@ -898,29 +922,47 @@ __device__ __forceinline__ void prestep_body(DevClock *clk, const Tables &T, int
 __global__ void k_prestep(DevClock *clk, Tables T, int fargo) { prestep_body(clk, T, fargo); }
 
 // simtime/drift/forces/kick/dump bookkeeping (main.cu:378-412)
-__device__ __forceinline__ void poststep_body(DevClock *clk, const Tables &T) {
+// phase 0: the whole end of a step; with a moving planet phase 1 (rotation,
+// time, drift, mass) and phase 2 (forces from the disk reductions f8, f9
+// made between the two, kick, bookkeeping; planet.cu:54-93, main.cu:378-412)
+__device__ __forceinline__ void poststep_body(DevClock *clk, const Tables &T, int phase = 0) {
   int t = threadIdx.x;
   DevClock &c = *clk;
   int halted = c.halted;
   __syncthreads();
   if (halted) return;
   // rotate_rings ppm.cu:309-322
-  for (int q = t; q < T.nr * T.nk; q += blockDim.x) {
+  for (int q = t; phase != 2 && q < T.nr * T.nk; q += blockDim.x) {
     int k = q / T.nr, i = q % T.nr;
     int rk = k * T.nrg + i + NPAD;
     T.rot_j[rk] = wrap1(T.rot_j[rk] + T.inc_j[rk], T.nphi);
   }
   if (t != 0) return;
   double dt = c.dt_step;
-  c.simtime += dt;
-  c.timem += dt;
-  c.ncycle += 1;
-  c.ncycp += 1;
-  if (c.plnt_flag > 0) {
-    d_drift(c.planet, c.frrot, dt, c);
+  if (phase != 2) {
+    c.simtime += dt;
+    c.timem += dt;
+    c.ncycle += 1;
+    c.ncycp += 1;
+  }
+  if (phase == 0) {
+    if (c.plnt_flag > 0) {
+      d_drift(c.planet, c.frrot, dt, c);
+      c.planet.m = d_set_M_p(c, c.simtime);
+      d_forces_fixed(c.planet, c.frrot);
+      d_kick(c.planet, c.frrot, 0.5 * dt, c.frrot_flag);
+    }
+  } else if (phase == 1) {
+    d_drift_moving(c.planet, c.frrot, dt, c);
     c.planet.m = d_set_M_p(c, c.simtime);
-    d_forces_fixed(c.planet, c.frrot);
-    d_kick(c.planet, c.frrot, 0.5 * dt, c.frrot_flag);
+    return;
+  } else {
+    // planet_forces planet.cu:58-59 with the disk sums of this state
+    Body &p = c.planet;
+    p.fx = c.Sigma_0 * c.f8 / p.m - 1.0 / p.x / p.x + p.x * pow(p.vy + c.frrot, 2);
+    p.fy = c.Sigma_0 * c.f9 / p.m;
+    d_kick(p, c.frrot, 0.5 * dt, c.frrot_flag);
+    c.frrot_next = c.frrot;      // the CFL of the next get_dt runs after this kernel
   }
   if (c.ncycp == c.nprin) { c.ncycp = 0; c.prin = 1; }
   if (c.make_pict) {
@@ -933,6 +975,8 @@ __device__ __forceinline__ void poststep_body(DevClock *clk, const Tables &T) {
 }
 
 __global__ void k_poststep(DevClock *clk, Tables T) { poststep_body(clk, T); }
+__global__ void k_poststep_drift(DevClock *clk, Tables T) { poststep_body(clk, T, 1); }
+__global__ void k_poststep_kick(DevClock *clk, Tables T) { poststep_body(clk, T, 2); }
 
 // ---------------------------------------------------------------------------
 // Batched 2D steps: one launch per phase walks the tiles of every run of a
@@ -1162,7 +1206,7 @@ void damp_clk(const Tables &T, double *r, double *u, double *v, double *w, const
 void cfl_clk(const Tables &T, const double *r, const double *u, const double *v, const double *w,
              const Phys &ph, DevClock *clk, cudaStream_t s) {
   dim3 grid(T.nr, T.nk);
-  k_cfl_clk<<<grid, 256, 0, s>>>(T, r, u, v, w, ph, clk);
+  k_cfl_clk<<<grid, 256, 0, s>>>(T, r, u, v, w, ph, clk, 3, 1);
 }
 
 void reduce(const Tables &T, const double *r, const Body &pl, const DevClock *clk, double exclude,
@@ -1183,6 +1227,29 @@ void reduce32(const Tables &T, const float *r, const Body &pl, const DevClock *c
 
 void prestep(DevClock *clk, const Tables &T, int fargo, cudaStream_t s) {
   k_prestep<<<1, 256, 0, s>>>(clk, T, fargo);
+}
+
+void poststep_drift(DevClock *clk, const Tables &T, cudaStream_t s) {
+  k_poststep_drift<<<1, 256, 0, s>>>(clk, T);
+}
+void poststep_kick(DevClock *clk, cudaStream_t s) {
+  Tables T{};
+  k_poststep_kick<<<1, 1, 0, s>>>(clk, T);
+}
+void reduce_forces(const Tables &T, const void *r, int fp32, DevClock *clk, double p_alpha, int ndim,
+                   double *ring_part, unsigned int *counter, cudaStream_t s) {
+  dim3 grid(T.nr, T.nk);
+  for (int mode : {8, 9}) {
+    if (fp32)
+      k_reduce_forces<float><<<grid, 1024, 0, s>>>(T, (const float *)r, clk, mode, p_alpha, ndim, ring_part, counter);
+    else
+      k_reduce_forces<double><<<grid, 1024, 0, s>>>(T, (const double *)r, clk, mode, p_alpha, ndim, ring_part, counter);
+  }
+}
+void cfl_clk_after(const Tables &T, const double *r, const double *u, const double *v, const double *w,
+                   const Phys &ph, DevClock *clk, int ndim, cudaStream_t s) {
+  dim3 grid(T.nr, T.nk);
+  k_cfl_clk<<<grid, 256, 0, s>>>(T, r, u, v, w, ph, clk, ndim, 0);
 }
 
 void poststep(DevClock *clk, const Tables &T, cudaStream_t s) {

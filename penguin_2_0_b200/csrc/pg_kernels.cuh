@@ -65,7 +65,8 @@ struct DevClock {
   int make_pict, prin, done, halted, status, pad;
   unsigned long long cfl_bits;   // max CFL rate as ordered bits (non-negative)
   int nprin, plnt_flag, frrot_flag, ndim;
-  double M_p, t_growth, rs_fac, sc2, R_p, Sigma_0;
+  double M_p, t_growth, rs_fac, sc2, R_p, Sigma_0, p_beta;
+  double f8, f9;                 // moving planet: disk forces of the step (reductions 8, 9)
   double hist_norm;
   double mass, torque;           // last diagnostics reductions
   double *hist;                  // device history rows (HIST_COLS each)
@@ -80,6 +81,7 @@ struct SweepCtl {
   DevClock *clk;      // non-null: read dt/planet/frrot from the clock, honour halt
   int fuse;           // sweepy epilogue: damping + CFL + finiteness check
   int shift;          // store at (j + inc_j) mod jmax: the last sweep of a step
+  int nocfl;          // with fuse: no CFL rate (a moving planet's FrRot is known only after the step)
 };
 
 // One run of a batch (pg_batch.cu): what its kernels read, in device memory.
@@ -136,7 +138,8 @@ void sweep_z32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCt
 void cfl32(const Tables &T, const Planes32 &cur, const Phys &ph, double frrot, int ndim, int rot_pending,
            unsigned long long *out, int *status, cudaStream_t s);
 void damp32(const Tables &T, const Planes32 &cur, double dt, const DevClock *clk, int ndim, cudaStream_t s);
-void cfl32_clk(const Tables &T, const Planes32 &cur, const Phys &ph, int ndim, DevClock *clk, cudaStream_t s);
+void cfl32_clk(const Tables &T, const Planes32 &cur, const Phys &ph, int ndim, DevClock *clk, cudaStream_t s,
+               int rot_pending = 1);
 // batched 2D steps over many runs (one launch per phase for all runs)
 void batch_prestep(const BatchRun *runs, int nruns, cudaStream_t s);
 void batch_poststep(const BatchRun *runs, int nruns, cudaStream_t s);
@@ -153,6 +156,13 @@ void damp_clk(const Tables &T, double *r, double *u, double *v, double *w, const
 void cfl_clk(const Tables &T, const double *r, const double *u, const double *v, const double *w,
              const Phys &ph, DevClock *clk, cudaStream_t s);
 void prestep(DevClock *clk, const Tables &T, int fargo, cudaStream_t s);
+// moving planet (plnt_flag 2): the step's end split around the disk-force reductions
+void poststep_drift(DevClock *clk, const Tables &T, cudaStream_t s);
+void poststep_kick(DevClock *clk, cudaStream_t s);
+void reduce_forces(const Tables &T, const void *r, int fp32, DevClock *clk, double p_alpha, int ndim,
+                   double *ring_part, unsigned int *counter, cudaStream_t s);
+void cfl_clk_after(const Tables &T, const double *r, const double *u, const double *v, const double *w,
+                   const Phys &ph, DevClock *clk, int ndim, cudaStream_t s);
 void poststep(DevClock *clk, const Tables &T, cudaStream_t s);
 void record(DevClock *clk, cudaStream_t s);
 }  // namespace pgk

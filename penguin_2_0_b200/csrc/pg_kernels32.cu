@@ -345,7 +345,8 @@ __device__ __forceinline__ void sweep_y32_body(ChunkShm32<NT> &S, double *red, c
     double m = block_max32(rate, red);
     int anybad = __syncthreads_or(bad);
     if (n == 0) {
-      if (m > 0.0 || m != m) atomicMax(&ctl.clk->cfl_bits, (unsigned long long)__double_as_longlong(m));
+      if (!ctl.nocfl && (m > 0.0 || m != m))
+        atomicMax(&ctl.clk->cfl_bits, (unsigned long long)__double_as_longlong(m));
       if (anybad) atomicExch(&ctl.clk->status, 3);
     }
   }
@@ -721,9 +722,10 @@ void cfl32(const Tables &T, const Planes32 &cur, const Phys &ph, double frrot, i
   k32_cfl<<<grid, 256, 0, s>>>(T, cur.r, cur.u, cur.v, cur.w, ph, frrot, ndim, rot_pending, out, status, nullptr);
 }
 
-void cfl32_clk(const Tables &T, const Planes32 &cur, const Phys &ph, int ndim, DevClock *clk, cudaStream_t s) {
+void cfl32_clk(const Tables &T, const Planes32 &cur, const Phys &ph, int ndim, DevClock *clk, cudaStream_t s,
+               int rot_pending) {
   dim3 grid(T.nr, T.nk);
-  k32_cfl<<<grid, 256, 0, s>>>(T, cur.r, cur.u, cur.v, cur.w, ph, 0.0, ndim, 1, nullptr, nullptr, clk);
+  k32_cfl<<<grid, 256, 0, s>>>(T, cur.r, cur.u, cur.v, cur.w, ph, 0.0, ndim, rot_pending, nullptr, nullptr, clk);
 }
 
 void damp32(const Tables &T, const Planes32 &cur, double dt, const DevClock *clk, int ndim, cudaStream_t s) {

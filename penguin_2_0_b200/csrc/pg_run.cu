@@ -814,7 +814,6 @@ int pg_clock_reset(pg_run *run, int startat) {
   if (!run) return PG_ERR_ARG;
   if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
   const pg_params &P = run->P;
-  if (P.plnt_flag == 2) return fail(run, PG_ERR_PARAMS, "the fused loop supports plnt_flag 0 and 1");
   if (P.ndim == 3 && run->nk > 64) return fail(run, PG_ERR_PARAMS, "3D diagnostics support kmax <= 64");
   CK(cudaSetDevice(run->dev));
   pgd::DevClock c{};
@@ -832,6 +831,7 @@ int pg_clock_reset(pg_run *run, int startat) {
   c.nprin = P.nprin; c.plnt_flag = P.plnt_flag; c.frrot_flag = P.FrRot_flag; c.ndim = P.ndim;
   c.M_p = P.M_p; c.t_growth = P.t_growth; c.rs_fac = P.rs_fac; c.sc2 = P.sc_h * P.sc_h; c.R_p = P.R_p;
   c.Sigma_0 = P.Sigma_0;
+  c.p_beta = P.p_beta;
   c.hist_norm = P.M_p * P.M_p * std::pow(P.R_p, 1.0 - P.p_alpha + (P.p_beta - 1.0)) / (P.sc_h * P.sc_h);
   c.hist = run->hist; c.hist_cap = run->hist_cap; c.hist_count = 0;
   cudaStream_t s = run->stream;
@@ -880,9 +880,11 @@ static int enqueue_step32(pg_run *run, pgd::SweepCtl c, int n, size_t e_step) {
   if (tm && ev_pair(run, 0, e_k)) return fail(run, PG_ERR_CUDA, "event record");
   pgk::sweep_x32(run->T, planes32_fwd(run, a), run->ph, c, P.ndim, s); n += nx(run);
   if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
+  const bool moving = P.plnt_flag == 2;
   if (P.ndim == 2) {
     c.fuse = 1;
     c.shift = 1;
+    c.nocfl = moving;
     if (tm && ev_pair(run, 1, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     pgk::sweep_y32(run->T, planes32_fwd(run, 1 - a), run->ph, c, 2, s); n += ny(run);
     if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
@@ -896,9 +898,18 @@ static int enqueue_step32(pg_run *run, pgd::SweepCtl c, int n, size_t e_step) {
     if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     run->cur = 1 - a;
     pgk::damp32(run->T, planes32_cur(run), 0.0, run->clk, 3, s); n++;
-    pgk::cfl32_clk(run->T, planes32_cur(run), run->ph, 3, run->clk, s); n++;
+    if (!moving) { pgk::cfl32_clk(run->T, planes32_cur(run), run->ph, 3, run->clk, s); n++; }
   }
-  pgk::poststep(run->clk, run->T, s); n++;
+  if (moving) {
+    // drift, disk forces on the drifted planet, kick; then the next CFL
+    pgk::poststep_drift(run->clk, run->T, s); n++;
+    pgk::reduce_forces(run->T, run->p32[run->cur][0], 1, run->clk, P.p_alpha, P.ndim, run->ring_part,
+                       run->counter, s); n += 2;
+    pgk::poststep_kick(run->clk, s); n++;
+    pgk::cfl32_clk(run->T, planes32_cur(run), run->ph, P.ndim, run->clk, s, 0); n++;
+  } else {
+    pgk::poststep(run->clk, run->T, s); n++;
+  }
   pgk::reduce32(run->T, run->p32[run->cur][0], pgd::Body{}, run->clk, 0.0, 0, P.plnt_flag > 0, P.p_alpha, P.ndim,
                 run->ring_part, run->counter, &run->clk->mass, s); n++;
   if (P.plnt_flag > 0 && P.ndim == 2) {
@@ -927,9 +938,11 @@ static int enqueue_step(pg_run *run, bool first_p0) {
   if (tm && ev_pair(run, 0, e_k)) return fail(run, PG_ERR_CUDA, "event record");
   pgk::sweep_x(run->T, planes_fwd(run, a, first_p0 ? run->p0 : nullptr), run->ph, c, P.ndim, s); n += nx(run);
   if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
+  const bool moving = P.plnt_flag == 2;
   if (P.ndim == 2) {
     c.fuse = 1;
     c.shift = 1;
+    c.nocfl = moving;
     if (tm && ev_pair(run, 1, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 2, s); n += ny(run);
     if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
@@ -944,10 +957,21 @@ static int enqueue_step(pg_run *run, bool first_p0) {
     if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     double **cp = run->planes[1 - a];
     pgk::damp_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->clk, s); n++;
-    pgk::cfl_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->ph, run->clk, s); n++;
+    if (!moving) { pgk::cfl_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->ph, run->clk, s); n++; }
     run->cur = 1 - a;
   }
-  pgk::poststep(run->clk, run->T, s); n++;
+  if (moving) {
+    // moving planet (planet.cu:54-93): drift, the disk's forces on the
+    // drifted planet (reductions 8 and 9), kick; FrRot is then known and the
+    // next get_dt's CFL runs on the stored state
+    double **cp = run->planes[run->cur];
+    pgk::poststep_drift(run->clk, run->T, s); n++;
+    pgk::reduce_forces(run->T, cp[0], 0, run->clk, P.p_alpha, P.ndim, run->ring_part, run->counter, s); n += 2;
+    pgk::poststep_kick(run->clk, s); n++;
+    pgk::cfl_clk_after(run->T, cp[0], cp[1], cp[2], cp[3], run->ph, run->clk, P.ndim, s); n++;
+  } else {
+    pgk::poststep(run->clk, run->T, s); n++;
+  }
   if (P.plnt_flag > 0 || true) {
     double **cp = run->planes[run->cur];
     pgk::reduce(run->T, cp[0], pgd::Body{}, run->clk, 0.0, 0, P.plnt_flag > 0, P.p_alpha, P.ndim,
@@ -1160,6 +1184,7 @@ int run_shape(const pg_run *run, RunShape *o) {
   o->loaded = run->loaded ? 1 : 0;
   o->clock_ready = run->clock_ready ? 1 : 0;
   o->p0_live = run->p0_live ? 1 : 0;
+  o->moving = run->P.plnt_flag == 2 ? 1 : 0;
   o->nr = run->nr; o->nphi = run->nphi; o->nk = run->nk;
   const pgd::Chunking &cx = run->T.cx;
   const bool short_last = !cx.stuck && cx.lim_last <= 64;

@@ -19,6 +19,7 @@ CASES = [
     dict(which=0, imax=128, jmax=384, M_p=1e-4, precision=1, ss_alpha=1e-2),
     dict(which=0, imax=136, jmax=408, plnt_flag=0, precision=1),
     dict(which=1, imax=64, jmax=132, kmax=16),
+    dict(which=0, imax=136, jmax=408, plnt_flag=2),             # moving planet: own launch sequence
 ]
 
 

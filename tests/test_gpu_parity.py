@@ -21,6 +21,7 @@ CASES = {
     "g120x150_plain": dict(imax=120, jmax=150, plnt_flag=0, visc_flag=0, flat_flag=0, FARGO_flag=0,
                            kill_rin=0.0, kill_rout=0.0),
     "cfg0": dict(imax=256, jmax=768),
+    "g136x136_moving": dict(imax=136, jmax=136, plnt_flag=2),   # the planet feels the disk (global.h default)
 }
 
 
@@ -108,3 +109,40 @@ def test_dump_roundtrip_bitwise(gpu):
         run.load(ic)
         out = run.save()
     assert bytes(out) == bytes(ic)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_moving_planet_fused_loop_matches_host_loop(gpu, precision):
+    # plnt_flag 2: the device loop drifts the planet, reduces the disk's
+    # forces on it (modes 8 and 9) and kicks it every step; the host-driven
+    # loop does the same through pg_planet_forces.  The softening rs = rs_fac
+    # h(x) uses the device pow on one side and the host pow on the other, so
+    # the two agree to rounding, not bit for bit.
+    p = _params(dict(imax=136, jmax=136, plnt_flag=2, precision=precision))
+    ic = pg.build_ic(p)
+    hist = []
+
+    def rec(s, simtime, dt_used, planet, FrRot):
+        hist.append((simtime, planet.x, planet.y, planet.vx, planet.vy))
+
+    with pg.Run(p, 0) as a, pg.Run(p, 0) as b:
+        a.load(ic)
+        b.load(ic)
+        a.kernel_loop(12, record=rec)
+        b.clock_reset(0)
+        assert b.advance(12) == 12
+        c, pl = b.clock()
+        t, x, y, vx, vy = hist[-1]
+        assert abs(c.simtime - t) <= 1e-12 * t
+        for got, want in ((pl.x, x), (pl.y, y)):
+            assert abs(got - want) <= 1e-12 * abs(want), (got, want)
+        for got, want in ((pl.vx, vx), (pl.vy, vy)):
+            assert abs(got - want) <= 1e-12 * max(abs(vx), abs(vy), 1e-6), (got, want)
+        fa, fb = pg.dump_fields(a.save(), p), pg.dump_fields(b.save(), p)
+        np.testing.assert_array_equal(fa["rot_j"], fb["rot_j"])
+        tol = 1e-12 if precision == 0 else 1e-6
+        speed = max(np.max(np.abs(fa["u"])), np.max(np.abs(fa["v"])))
+        assert rel_linf(fb["r"], fa["r"]) <= tol
+        assert np.max(np.abs(fb["u"] - fa["u"])) / speed <= tol
+        assert np.max(np.abs(fb["v"] - fa["v"])) / speed <= tol

@@ -266,6 +266,20 @@ int pg_reduce_noalloc(const double *sigma, int64_t row_stride, const double *xc,
                       double exclude, int mode, double p_alpha, double sc_h,
                       double *out, void *stream);
 
+/* ---- post-processing (the reference's read/ tools) on the device ----------
+ * Both read the run's current state in physical azimuth order, which is what
+ * read/p_init.cpp:108-133 (update_grid) reconstructs from a dump by undoing
+ * each ring's rot_j; load a dump with pg_load_dump to process it.
+ * pg_post_harmonic: read/p_output.cpp:35-55 (write_har_file) for layer 0,
+ *   an[i] = sum_j sin(m yc_j) Sigma_ij, bn[i] = sum_j cos(m yc_j) Sigma_ij,
+ *   an, bn host arrays of imax doubles.
+ * pg_post_torque: read/transform.cpp:386-420 (get_torque), the disk's torque
+ *   on a planet of mass ratio M_p at r = 1, azimuth pi, barycentric frame.
+ * Sums run in a different order from the reference's sequential loops, so
+ * they agree to rounding.                                                     */
+int pg_post_harmonic(pg_run *run, double m, double *an, double *bn);
+int pg_post_torque(pg_run *run, double M_p, double *out);
+
 /* ---- batches: many disks stepped together --------------------------------
  * No counterpart in the reference (one disk per process).  A batch steps its
  * member runs together: per step, one launch per phase walks the pencil

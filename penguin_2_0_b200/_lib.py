@@ -170,6 +170,8 @@ def lib() -> C.CDLL:
         "pg_batch_launch_count": (C.c_int64, [vp]),
         "pg_batch_stream": (vp, [vp]),
         "pg_run_device_bytes": (C.c_size_t, [P]),
+        "pg_post_harmonic": (C.c_int, [vp, C.c_double, dp, dp]),
+        "pg_post_torque": (C.c_int, [vp, C.c_double, dp]),
         "pg_server_create": (C.c_int, [C.c_int, C.c_size_t, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
         "pg_server_destroy": (C.c_int, [vp]),
         "pg_server_last_error": (C.c_char_p, [vp]),

@@ -979,6 +979,68 @@ __global__ void k_poststep_drift(DevClock *clk, Tables T) { poststep_body(clk, T
 __global__ void k_poststep_kick(DevClock *clk, Tables T) { poststep_body(clk, T, 2); }
 
 // ---------------------------------------------------------------------------
+// Post-processing of a state (the reference's read/ tools, on the device).
+// Both work on the physical-order planes, which is what read/p_init.cpp:108-133
+// (update_grid) builds from a dump by undoing each ring's rot_j.
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+  return t;
+}
+
+// write_har_file, read/p_output.cpp:35-55: per ring of layer 0,
+// a = sum_j sin(m yc_j) Sigma_j and b = sum_j cos(m yc_j) Sigma_j
+template <typename RT>
+__global__ void k_post_harmonic(Tables T, const RT *R, double m, double *ab) {
+  __shared__ double red[32];
+  const int i = blockIdx.x, rk = i + NPAD;
+  const size_t base = (size_t)rk * T.nphi;
+  const double off = (sizeof(RT) == 4) ? T.sbg[rk] : 0.0;   // FP32 planes hold Sigma - S_bg
+  double a = 0.0, b = 0.0;
+  for (int j = threadIdx.x; j < T.nphi; j += blockDim.x) {
+    double sig = off + (double)R[base + j];
+    a += sin(m * T.yc[j]) * sig;
+    b += cos(m * T.yc[j]) * sig;
+  }
+  a = block_sum(a, red);
+  b = block_sum(b, red);
+  if (threadIdx.x == 0) { ab[2 * i] = a; ab[2 * i + 1] = b; }
+}
+
+// get_torque, read/transform.cpp:386-420: torque of the disk on a planet of
+// mass ratio M_p at r = 1, azimuth pi, in the barycentric frame (star at
+// distance M_p/(1+M_p) opposite), softening 3e-6 in Rp^2; one sum per ring
+template <typename RT>
+__global__ void k_post_torque(Tables T, const RT *R, double M_p, double *ring_out) {
+  __shared__ double red[32];
+  const int i = blockIdx.x, k = blockIdx.y;
+  const int row = i + NPAD, rk = k * T.nrg + row, kz = k + NPAD;
+  const size_t base = (size_t)rk * T.nphi;
+  const double off = (sizeof(RT) == 4) ? T.sbg[rk] : 0.0;
+  const double stm = 1.0 / (1.0 + M_p), plm = M_p * stm, plx = 1.0 * stm, stx = 1.0 * plm;
+  const double rad = T.rxc[row], z = T.zc[kz], dxz = T.rdx[row] * T.dz[kz];
+  double t = 0.0;
+  for (int j = threadIdx.x; j < T.nphi; j += blockDim.x) {
+    double azi = T.yc[j];
+    double cosfac = cos(azi - 3.1415926535897932384626433832795);
+    double sinfac = sin(azi - 3.1415926535897932384626433832795);
+    double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac + z * z;
+    Rp = sqrt(Rp + 0.000003);
+    double Rs = sqrt(rad * rad + stx * stx + 2.0 * stx * rad * cosfac + z * z);
+    double rho = off + (double)R[base + j];
+    t += rho * (plm * plx * sinfac / (Rp * Rp * Rp) - stm * stx * sinfac / (Rs * Rs * Rs)) * rad * T.dy[j] * dxz;
+  }
+  t = block_sum(t, red);
+  if (threadIdx.x == 0) ring_out[k * T.nr + i] = t;
+}
+
+// ---------------------------------------------------------------------------
 // Batched 2D steps: one launch per phase walks the tiles of every run of a
 // group.  A tile is one pencil chunk (sweeps) or one ring (reductions); the
 // run of tile t is found by bisection in the queue's prefix sums.  Each
@@ -1250,6 +1312,16 @@ void cfl_clk_after(const Tables &T, const double *r, const double *u, const doub
                    const Phys &ph, DevClock *clk, int ndim, cudaStream_t s) {
   dim3 grid(T.nr, T.nk);
   k_cfl_clk<<<grid, 256, 0, s>>>(T, r, u, v, w, ph, clk, ndim, 0);
+}
+
+void post_harmonic(const Tables &T, const void *r, int fp32, double m, double *ab, cudaStream_t s) {
+  if (fp32) k_post_harmonic<float><<<T.nr, 256, 0, s>>>(T, (const float *)r, m, ab);
+  else k_post_harmonic<double><<<T.nr, 256, 0, s>>>(T, (const double *)r, m, ab);
+}
+void post_torque(const Tables &T, const void *r, int fp32, double M_p, double *ring_out, cudaStream_t s) {
+  dim3 grid(T.nr, T.nk);
+  if (fp32) k_post_torque<float><<<grid, 256, 0, s>>>(T, (const float *)r, M_p, ring_out);
+  else k_post_torque<double><<<grid, 256, 0, s>>>(T, (const double *)r, M_p, ring_out);
 }
 
 void poststep(DevClock *clk, const Tables &T, cudaStream_t s) {

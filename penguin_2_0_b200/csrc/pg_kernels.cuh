@@ -164,5 +164,9 @@ void reduce_forces(const Tables &T, const void *r, int fp32, DevClock *clk, doub
 void cfl_clk_after(const Tables &T, const double *r, const double *u, const double *v, const double *w,
                    const Phys &ph, DevClock *clk, int ndim, cudaStream_t s);
 void poststep(DevClock *clk, const Tables &T, cudaStream_t s);
+// post-processing (read/ tools): azimuthal harmonic m per ring of layer 0
+// (ab[2i], ab[2i+1]), torque on a planet at r = 1 per ring (ring_out[k*nr+i])
+void post_harmonic(const Tables &T, const void *r, int fp32, double m, double *ab, cudaStream_t s);
+void post_torque(const Tables &T, const void *r, int fp32, double M_p, double *ring_out, cudaStream_t s);
 void record(DevClock *clk, cudaStream_t s);
 }  // namespace pgk

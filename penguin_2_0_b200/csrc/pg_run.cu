@@ -1156,6 +1156,52 @@ int pg_history(pg_run *run, double *rows, int max, int *rows_out) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// post-processing of the current state (read/ tools)
+static int post_buffer(pg_run *run, size_t n, double **buf) {
+  if (cudaMalloc(buf, n * sizeof(double)) != cudaSuccess) return fail(run, PG_ERR_NOMEM, "post-processing buffer");
+  return PG_OK;
+}
+
+extern "C" int pg_post_harmonic(pg_run *run, double m, double *an, double *bn) {
+  if (!run || !an || !bn) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  CK(cudaSetDevice(run->dev));
+  double *ab = nullptr;
+  if (int e = post_buffer(run, 2 * (size_t)run->nr, &ab)) return e;
+  const void *r = run->fp32 ? (const void *)run->p32[run->cur][0] : (const void *)run->planes[run->cur][0];
+  pgk::post_harmonic(run->T, r, run->fp32, m, ab, run->stream);
+  std::vector<double> h(2 * (size_t)run->nr);
+  cudaError_t e1 = cudaGetLastError();
+  cudaError_t e2 = cudaMemcpyAsync(h.data(), ab, h.size() * sizeof(double), cudaMemcpyDeviceToHost, run->stream);
+  cudaError_t e3 = cudaStreamSynchronize(run->stream);
+  cudaFree(ab);
+  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) return fail(run, PG_ERR_CUDA, "post_harmonic");
+  for (int i = 0; i < run->nr; i++) { an[i] = h[2 * i]; bn[i] = h[2 * i + 1]; }
+  return PG_OK;
+}
+
+extern "C" int pg_post_torque(pg_run *run, double M_p, double *out) {
+  if (!run || !out) return PG_ERR_ARG;
+  if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
+  CK(cudaSetDevice(run->dev));
+  size_t n = (size_t)run->nr * run->nk;
+  double *rb = nullptr;
+  if (int e = post_buffer(run, n, &rb)) return e;
+  const void *r = run->fp32 ? (const void *)run->p32[run->cur][0] : (const void *)run->planes[run->cur][0];
+  pgk::post_torque(run->T, r, run->fp32, M_p, rb, run->stream);
+  std::vector<double> h(n);
+  cudaError_t e1 = cudaGetLastError();
+  cudaError_t e2 = cudaMemcpyAsync(h.data(), rb, n * sizeof(double), cudaMemcpyDeviceToHost, run->stream);
+  cudaError_t e3 = cudaStreamSynchronize(run->stream);
+  cudaFree(rb);
+  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) return fail(run, PG_ERR_CUDA, "post_torque");
+  double t = 0.0;
+  for (size_t q = 0; q < n; q++) t += h[q];
+  *out = t;
+  return PG_OK;
+}
+
+// ---------------------------------------------------------------------------
 // device footprint of a run (pg_create's allocations), for admission control
 extern "C" size_t pg_run_device_bytes(const pg_params *p) {
   if (!p) return 0;

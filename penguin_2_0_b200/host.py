@@ -181,6 +181,21 @@ class Run:
         """pg_save_rings into a raw host pointer (e.g. a pinned buffer)."""
         _check(_lib.lib().pg_save_rings(self._h, C.c_void_p(ptr), nbytes), self, "pg_save_rings")
 
+    def harmonic(self, m: float) -> tuple[np.ndarray, np.ndarray]:
+        """Azimuthal harmonic m of Sigma per ring of layer 0 (read/ write_har_file)."""
+        an = np.zeros(self.p.imax)
+        bn = np.zeros(self.p.imax)
+        dp = C.POINTER(C.c_double)
+        _check(_lib.lib().pg_post_harmonic(self._h, m, an.ctypes.data_as(dp), bn.ctypes.data_as(dp)), self,
+               "pg_post_harmonic")
+        return an, bn
+
+    def post_torque(self, M_p: float) -> float:
+        """Disk torque on a planet at r = 1, azimuth pi (read/ get_torque)."""
+        out = C.c_double(0.0)
+        _check(_lib.lib().pg_post_torque(self._h, M_p, C.byref(out)), self, "pg_post_torque")
+        return out.value
+
     def load_dump(self, path: str) -> "Run":
         _check(_lib.lib().pg_load_dump(self._h, path.encode()), self, "pg_load_dump")
         return self

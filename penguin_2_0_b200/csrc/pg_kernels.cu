@@ -979,6 +979,94 @@ __global__ void k_poststep_drift(DevClock *clk, Tables T) { poststep_body(clk, T
 __global__ void k_poststep_kick(DevClock *clk, Tables T) { poststep_body(clk, T, 2); }
 
 // ---------------------------------------------------------------------------
+// Dump <-> planes.  The dump holds each ring's field arrays in storage order
+// (j_store = j_phys - rot_j, init.cpp:241, output.cu:48-55); the planes hold
+// physical order.  Thread (j, ring i, layer k) moves one cell.
+__global__ void k_unpack_dump(Tables T, const double *stage, DumpPlanes D, int ndim, int fp32, int *err) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y, k = blockIdx.z;
+  const int nphi = T.nphi;
+  if (j >= nphi) return;
+  const int rk = k * T.nrg + i + NPAD;
+  int jp = j + T.rot_j[rk];
+  if (jp >= nphi) jp -= nphi;
+  const double *f = stage + ((size_t)i + (size_t)T.nr * k) * 5 * nphi;
+  const double r = f[j], p = f[nphi + j], u = f[2 * nphi + j], v = f[3 * nphi + j], w = f[4 * nphi + j];
+  if (!(r > 0.0) || !isfinite(r)) atomicOr(err, 1);
+  if (ndim == 2 && w != 0.0) atomicOr(err, 2);
+  const size_t o = (size_t)rk * nphi + jp;
+  if (fp32) {
+    D.fr[o] = (float)(r - T.sbg[rk]);
+    D.fu[o] = (float)u;
+    D.fv[o] = (float)(v - T.vbg[rk]);
+    if (ndim == 3) D.fw[o] = (float)w;
+  } else {
+    D.r[o] = r; D.u[o] = u; D.v[o] = v; D.p0[o] = p;
+    if (ndim == 3) D.w[o] = w;
+  }
+}
+
+// the fixed radial ghost rings (init_bound, init.cpp:253-413): phi-uniform
+// r, u, v, p per ghost row, w = 0
+__global__ void k_fill_ghost_rows(Tables T, const double *ghosts, DumpPlanes D, int ndim, int fp32) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, gi = blockIdx.y, k = blockIdx.z;
+  if (j >= T.nphi) return;
+  const int row = gi < NPAD ? gi : T.nr + gi;
+  const int rk = k * T.nrg + row;
+  const double *g = ghosts + ((size_t)k * 2 * NPAD + gi) * 4;
+  const size_t o = (size_t)rk * T.nphi + j;
+  if (fp32) {
+    D.fr[o] = (float)(g[0] - T.sbg[rk]);
+    D.fu[o] = (float)g[1];
+    D.fv[o] = (float)(g[2] - T.vbg[rk]);
+    if (ndim == 3) D.fw[o] = 0.f;
+  } else {
+    D.r[o] = g[0]; D.u[o] = g[1]; D.v[o] = g[2]; D.p0[o] = g[3];
+    if (ndim == 3) D.w[o] = 0.0;
+  }
+}
+
+// whole ring records (72*nphi + 96 bytes) in the dump layout
+__global__ void k_pack_dump(Tables T, DumpPlanes D, int ndim, int fp32, int p0_live, unsigned char *out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y, k = blockIdx.z;
+  const int nphi = T.nphi, row = i + NPAD, rk = k * T.nrg + row, kz = k + NPAD;
+  if (j >= nphi) return;
+  unsigned char *base = out + ((size_t)i + (size_t)T.nr * k) * ((size_t)72 * nphi + 96);
+  int jp = j + T.rot_j[rk];
+  if (jp >= nphi) jp -= nphi;
+  const size_t o = (size_t)rk * nphi + jp;
+  double *f = (double *)base;
+  double r, u, v, w;
+  if (fp32) {
+    r = T.sbg[rk] + (double)D.fr[o];
+    u = D.fu[o];
+    v = T.vbg[rk] + (double)D.fv[o];
+    w = (ndim == 3) ? (double)D.fw[o] : 0.0;
+  } else {
+    r = D.r[o]; u = D.u[o]; v = D.v[o];
+    w = (ndim == 3) ? D.w[o] : 0.0;
+  }
+  f[j] = r;
+  f[nphi + j] = p0_live ? D.p0[o] : r * T.cs2[rk];   // EOS-0 store, ppm.cu:139
+  f[2 * nphi + j] = u;
+  f[3 * nphi + j] = v;
+  f[4 * nphi + j] = w;
+  double *col = (double *)(base + (size_t)40 * nphi + 32);
+  col[j] = T.y[j]; col[nphi + j] = T.dy[j]; col[2 * nphi + j] = T.yvol[j]; col[3 * nphi + j] = T.yc[j];
+  if (j == 0) {
+    double *sc = (double *)(base + (size_t)40 * nphi);
+    sc[0] = T.rx[row]; sc[1] = T.rdx[row]; sc[2] = T.rxvol[row]; sc[3] = T.rxc[row];
+    double *zs = (double *)(base + (size_t)72 * nphi + 32);
+    zs[0] = T.z[kz]; zs[1] = T.dz[kz]; zs[2] = T.zvol[kz]; zs[3] = T.zc[kz];
+    int *ik = (int *)(base + (size_t)72 * nphi + 64);
+    ik[0] = i; ik[1] = k;
+    double *rot = (double *)(base + (size_t)72 * nphi + 72);
+    rot[0] = T.rot_v[rk]; rot[1] = T.res_v[rk];
+    int *rj = (int *)(base + (size_t)72 * nphi + 88);
+    rj[0] = T.rot_j[rk]; rj[1] = T.inc_j[rk];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Post-processing of a state (the reference's read/ tools, on the device).
 // Both work on the physical-order planes, which is what read/p_init.cpp:108-133
 // (update_grid) builds from a dump by undoing each ring's rot_j.
@@ -1322,6 +1410,22 @@ void post_torque(const Tables &T, const void *r, int fp32, double M_p, double *r
   dim3 grid(T.nr, T.nk);
   if (fp32) k_post_torque<float><<<grid, 256, 0, s>>>(T, (const float *)r, M_p, ring_out);
   else k_post_torque<double><<<grid, 256, 0, s>>>(T, (const double *)r, M_p, ring_out);
+}
+
+void unpack_dump(const Tables &T, const double *stage, const DumpPlanes &D, int ndim, int fp32, int *err,
+                 cudaStream_t s) {
+  dim3 grid((T.nphi + 255) / 256, T.nr, T.nk);
+  k_unpack_dump<<<grid, 256, 0, s>>>(T, stage, D, ndim, fp32, err);
+}
+void fill_ghost_rows(const Tables &T, const double *ghosts, const DumpPlanes &D, int ndim, int fp32,
+                     cudaStream_t s) {
+  dim3 grid((T.nphi + 255) / 256, 2 * NPAD, T.nk);
+  k_fill_ghost_rows<<<grid, 256, 0, s>>>(T, ghosts, D, ndim, fp32);
+}
+void pack_dump(const Tables &T, const DumpPlanes &D, int ndim, int fp32, int p0_live, unsigned char *out,
+               cudaStream_t s) {
+  dim3 grid((T.nphi + 255) / 256, T.nr, T.nk);
+  k_pack_dump<<<grid, 256, 0, s>>>(T, D, ndim, fp32, p0_live, out);
 }
 
 void poststep(DevClock *clk, const Tables &T, cudaStream_t s) {

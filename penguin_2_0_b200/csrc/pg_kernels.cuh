@@ -84,6 +84,12 @@ struct SweepCtl {
   int nocfl;          // with fuse: no CFL rate (a moving planet's FrRot is known only after the step)
 };
 
+// Planes a dump is unpacked into / packed from (pg_load_rings, pg_save_rings).
+struct DumpPlanes {
+  double *r, *u, *v, *w, *p0;    // FP64 run, p0: the dump's pressure
+  float *fr, *fu, *fv, *fw;      // FP32 run (residual Sigma and v_phi)
+};
+
 // One run of a batch (pg_batch.cu): what its kernels read, in device memory.
 struct BatchRun {
   Tables T;
@@ -164,6 +170,15 @@ void reduce_forces(const Tables &T, const void *r, int fp32, DevClock *clk, doub
 void cfl_clk_after(const Tables &T, const double *r, const double *u, const double *v, const double *w,
                    const Phys &ph, DevClock *clk, int ndim, cudaStream_t s);
 void poststep(DevClock *clk, const Tables &T, cudaStream_t s);
+// dump <-> planes: stage holds the dump's field arrays ring by ring ([nr*nk][5][nphi]
+// for unpack, whole 72*nphi+96-byte ring records for pack); err bit 1: a density
+// that is not finite and positive, bit 2: nonzero w in a 2D dump
+void unpack_dump(const Tables &T, const double *stage, const DumpPlanes &D, int ndim, int fp32, int *err,
+                 cudaStream_t s);
+void fill_ghost_rows(const Tables &T, const double *ghosts, const DumpPlanes &D, int ndim, int fp32,
+                     cudaStream_t s);
+void pack_dump(const Tables &T, const DumpPlanes &D, int ndim, int fp32, int p0_live, unsigned char *out,
+               cudaStream_t s);
 // post-processing (read/ tools): azimuthal harmonic m per ring of layer 0
 // (ab[2i], ab[2i+1]), torque on a planet at r = 1 per ring (ring_out[k*nr+i])
 void post_harmonic(const Tables &T, const void *r, int fp32, double m, double *ab, cudaStream_t s);

@@ -57,9 +57,6 @@ struct pg_run {
   double *hist = nullptr;
   int hist_cap = 4096;
   // host side
-  std::vector<unsigned char> tmpl;   // last loaded dump (geometry fields)
-  std::vector<double> h_vbg, h_sbg;
-  std::vector<double> h_cs2;
   bool loaded = false;
   bool clock_ready = false;
   int64_t launches = 0;
@@ -360,40 +357,16 @@ int pg_load_rings(pg_run *run, const void *rings, size_t bytes) {
         q[0] = tp.r; q[1] = tp.p; q[2] = tp.u; q[3] = tp.v;
       }
   }
-  // planes in physical azimuth order
-  const size_t pe = run->plane_elems;
-  std::vector<double> hr(pe), hu(pe), hv(pe), hw(P.ndim == 3 ? pe : 0), hp(pe, 0.0);
-  for (int k = 0; k < nk; k++) {
+  // ghost rows: phi-uniform r, u, v, p of each fixed radial ghost ring
+  std::vector<double> gh((size_t)nk * 2 * NPAD * 4);
+  for (int k = 0; k < nk; k++)
     for (int gi = 0; gi < NPAD; gi++) {
       const pg::GhostRing *gs[2] = {&lft[gi + NPAD * k], &rgh[gi + NPAD * k]};
-      int rows[2] = {gi, nr + NPAD + gi};
-      for (int s = 0; s < 2; s++) {
-        size_t off = ((size_t)k * nrg + rows[s]) * nphi;
-        for (int j = 0; j < nphi; j++) {
-          hr[off + j] = gs[s]->r; hu[off + j] = gs[s]->u; hv[off + j] = gs[s]->v; hp[off + j] = gs[s]->p;
-          if (P.ndim == 3) hw[off + j] = 0.0;
-        }
+      for (int sd = 0; sd < 2; sd++) {
+        double *q = &gh[(((size_t)k * 2 * NPAD) + gi + sd * NPAD) * 4];
+        q[0] = gs[sd]->r; q[1] = gs[sd]->u; q[2] = gs[sd]->v; q[3] = gs[sd]->p;
       }
     }
-    for (int i = 0; i < nr; i++) {
-      size_t rk = (size_t)k * nrg + i + NPAD;
-      size_t off = rk * nphi;
-      pg::RingView rv((unsigned char *)b + rb * (i + (size_t)nr * k), nphi);
-      int rj = rot_j[rk];
-      for (int js = 0; js < nphi; js++) {
-        int jp = js + rj;
-        if (jp >= nphi) jp -= nphi;
-        hr[off + jp] = rv.f(0)[js];
-        hp[off + jp] = rv.f(1)[js];
-        hu[off + jp] = rv.f(2)[js];
-        hv[off + jp] = rv.f(3)[js];
-        double w = rv.f(4)[js];
-        if (P.ndim == 3) hw[off + jp] = w;
-        else if (w != 0.0) return fail(run, PG_ERR_STATE, "2D dump with nonzero w");
-        if (!(rv.f(0)[js] > 0.0) || !std::isfinite(rv.f(0)[js])) return fail(run, PG_ERR_STATE, "non-positive density in dump");
-      }
-    }
-  }
   cudaStream_t s = run->stream;
   pgd::Tables &T = run->T;
   auto up = [&](const double *dst, const std::vector<double> &src) {
@@ -407,42 +380,51 @@ int pg_load_rings(pg_run *run, const void *rings, size_t bytes) {
   CK(up(T.y, g.zya)); CK(up(T.dy, g.zdy)); CK(up(T.yvol, g.yvol)); CK(up(T.yc, g.zyc));
   CK(up(T.z, z)); CK(up(T.dz, dz)); CK(up(T.zvol, zvol)); CK(up(T.zc, zc));
   CK(up(T.tg, tg));
-  std::vector<float> fr, fu, fv, fw;
-  if (run->fp32) {
-    // FP32 planes: Sigma, v_r, dv = v_phi - v_bg(ring), v_theta
-    fr.resize(pe); fu.resize(pe); fv.resize(pe);
-    if (P.ndim == 3) fw.resize(pe);
-    for (size_t rkq = 0; rkq < nring; rkq++)
-      for (int j = 0; j < nphi; j++) {
-        size_t q = rkq * nphi + j;
-        fr[q] = (float)(hr[q] - sbg[rkq]); fu[q] = (float)hu[q]; fv[q] = (float)(hv[q] - vbg[rkq]);
-        if (P.ndim == 3) fw[q] = (float)hw[q];
-      }
-    for (int bsel = 0; bsel < 2; bsel++) {
-      CK(cudaMemcpyAsync(run->p32[bsel][0], fr.data(), pe * sizeof(float), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(run->p32[bsel][1], fu.data(), pe * sizeof(float), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(run->p32[bsel][2], fv.data(), pe * sizeof(float), cudaMemcpyHostToDevice, s));
-      if (P.ndim == 3)
-        CK(cudaMemcpyAsync(run->p32[bsel][3], fw.data(), pe * sizeof(float), cudaMemcpyHostToDevice, s));
-    }
-  } else {
-    for (int bsel = 0; bsel < 2; bsel++) {
-      CK(cudaMemcpyAsync(run->planes[bsel][0], hr.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(run->planes[bsel][1], hu.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(run->planes[bsel][2], hv.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
-      if (P.ndim == 3)
-        CK(cudaMemcpyAsync(run->planes[bsel][3], hw.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
-    }
-    CK(cudaMemcpyAsync(run->p0, hp.data(), pe * sizeof(double), cudaMemcpyHostToDevice, s));
+  // the dump's field arrays (the first 40*nphi bytes of each ring record) go
+  // to the device as they are and are de-rotated into the planes there
+  const size_t pe = run->plane_elems;
+  const size_t fbytes = (size_t)40 * nphi;
+  double *stage = nullptr, *dgh = nullptr;
+  int *derr = nullptr;
+  auto release = [&]() { cudaFree(stage); cudaFree(dgh); cudaFree(derr); };
+  if (cudaMalloc(&stage, fbytes * nr * nk) != cudaSuccess || cudaMalloc(&dgh, gh.size() * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&derr, sizeof(int)) != cudaSuccess) {
+    release();
+    return fail(run, PG_ERR_NOMEM, "dump staging buffer");
   }
+  cudaError_t ce = cudaMemsetAsync(derr, 0, sizeof(int), s);
+  if (ce == cudaSuccess) ce = cudaMemcpy2DAsync(stage, fbytes, b, rb, fbytes, (size_t)nr * nk, cudaMemcpyHostToDevice, s);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(dgh, gh.data(), gh.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+  pgd::DumpPlanes D{};
+  if (run->fp32) {
+    D.fr = run->p32[0][0]; D.fu = run->p32[0][1]; D.fv = run->p32[0][2]; D.fw = run->p32[0][3];
+  } else {
+    D.r = run->planes[0][0]; D.u = run->planes[0][1]; D.v = run->planes[0][2]; D.w = run->planes[0][3];
+    D.p0 = run->p0;
+  }
+  if (ce == cudaSuccess) {
+    pgk::unpack_dump(T, stage, D, P.ndim, run->fp32, derr, s);
+    pgk::fill_ghost_rows(T, dgh, D, P.ndim, run->fp32, s);
+    ce = cudaGetLastError();
+  }
+  // the second plane copy starts equal to the first (ghost rows included)
+  int nf = (P.ndim == 3) ? 4 : 3;
+  for (int f = 0; f < nf && ce == cudaSuccess; f++) {
+    if (run->fp32) ce = cudaMemcpyAsync(run->p32[1][f], run->p32[0][f], pe * sizeof(float), cudaMemcpyDeviceToDevice, s);
+    else ce = cudaMemcpyAsync(run->planes[1][f], run->planes[0][f], pe * sizeof(double), cudaMemcpyDeviceToDevice, s);
+  }
+  int herr = 0;
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+  release();
+  if (ce != cudaSuccess) return fail(run, PG_ERR_CUDA, std::string("dump upload: ") + cudaGetErrorString(ce));
+  run->loaded = false;
+  if (herr & 1) return fail(run, PG_ERR_STATE, "non-positive density in dump");
+  if (herr & 2) return fail(run, PG_ERR_STATE, "2D dump with nonzero w");
+  run->launches += 2;
   pgk::tables(T, run->ph, P.ndim, P.kill_rin, P.kill_rout, P.xmin, P.xmax, s);
   if (int e = check_launch(run, 1)) return e;
   CK(cudaStreamSynchronize(s));
-  run->h_cs2.resize(nring);
-  CK(cudaMemcpy(run->h_cs2.data(), T.cs2, nring * sizeof(double), cudaMemcpyDeviceToHost));
-  run->h_vbg = vbg;
-  run->h_sbg = sbg;
-  run->tmpl.assign(b, b + bytes);
   run->cur = 0;
   run->p0_live = !run->fp32;
   run->loaded = true;
@@ -471,66 +453,26 @@ int pg_save_rings(pg_run *run, void *rings, size_t bytes) {
   size_t rb = pg::ring_bytes(P.jmax);
   if (bytes != rb * (size_t)P.imax * P.kmax) return fail(run, PG_ERR_ARG, "buffer size mismatch");
   CK(cudaSetDevice(run->dev));
-  const int nr = run->nr, nphi = run->nphi, nk = run->nk, nrg = run->nrg;
-  const size_t nring = (size_t)nk * nrg, pe = run->plane_elems;
-  std::vector<double> hr(pe), hu(pe), hv(pe), hw(P.ndim == 3 ? pe : 0), hp;
-  std::vector<double> res_v(nring), rot_v(nring);
-  std::vector<int> inc_j(nring), rot_j(nring);
+  // the whole dump is assembled on the device (fields in storage order,
+  // p = Sigma cs2, geometry, rot/inc) and copied back in one transfer
   cudaStream_t s = run->stream;
-  std::vector<float> fr, fu, fv, fw;
+  unsigned char *stage = nullptr;
+  if (cudaMalloc(&stage, bytes) != cudaSuccess) return fail(run, PG_ERR_NOMEM, "dump staging buffer");
+  pgd::DumpPlanes D{};
+  const int c = run->cur;
   if (run->fp32) {
-    float **fp = run->p32[run->cur];
-    fr.resize(pe); fu.resize(pe); fv.resize(pe);
-    if (P.ndim == 3) fw.resize(pe);
-    CK(cudaMemcpyAsync(fr.data(), fp[0], pe * sizeof(float), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(fu.data(), fp[1], pe * sizeof(float), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(fv.data(), fp[2], pe * sizeof(float), cudaMemcpyDeviceToHost, s));
-    if (P.ndim == 3) CK(cudaMemcpyAsync(fw.data(), fp[3], pe * sizeof(float), cudaMemcpyDeviceToHost, s));
+    D.fr = run->p32[c][0]; D.fu = run->p32[c][1]; D.fv = run->p32[c][2]; D.fw = run->p32[c][3];
   } else {
-    double **cp = run->planes[run->cur];
-    CK(cudaMemcpyAsync(hr.data(), cp[0], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(hu.data(), cp[1], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(hv.data(), cp[2], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (P.ndim == 3) CK(cudaMemcpyAsync(hw.data(), cp[3], pe * sizeof(double), cudaMemcpyDeviceToHost, s));
+    D.r = run->planes[c][0]; D.u = run->planes[c][1]; D.v = run->planes[c][2]; D.w = run->planes[c][3];
+    D.p0 = run->p0;
   }
-  if (run->p0_live) {
-    hp.resize(pe);
-    CK(cudaMemcpyAsync(hp.data(), run->p0, pe * sizeof(double), cudaMemcpyDeviceToHost, s));
-  }
-  CK(cudaMemcpyAsync(res_v.data(), run->T.res_v, nring * sizeof(double), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(rot_v.data(), run->T.rot_v, nring * sizeof(double), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(inc_j.data(), run->T.inc_j, nring * sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(rot_j.data(), run->T.rot_j, nring * sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
-  if (run->fp32) {
-    for (size_t rkq = 0; rkq < nring; rkq++)
-      for (int j = 0; j < nphi; j++) {
-        size_t q = rkq * nphi + j;
-        hr[q] = run->h_sbg[rkq] + (double)fr[q]; hu[q] = fu[q]; hv[q] = run->h_vbg[rkq] + (double)fv[q];
-        if (P.ndim == 3) hw[q] = fw[q];
-      }
-  }
-  unsigned char *out = (unsigned char *)rings;
-  std::memcpy(out, run->tmpl.data(), bytes);
-  for (int k = 0; k < nk; k++)
-    for (int i = 0; i < nr; i++) {
-      size_t rk = (size_t)k * nrg + i + NPAD, off = rk * nphi;
-      pg::RingView rv(out + rb * (i + (size_t)nr * k), nphi);
-      int rj = rot_j[rk];
-      double c2 = run->h_cs2[rk];
-      for (int js = 0; js < nphi; js++) {
-        int jp = js + rj;
-        if (jp >= nphi) jp -= nphi;
-        double r = hr[off + jp];
-        rv.f(0)[js] = r;
-        rv.f(1)[js] = run->p0_live ? hp[off + jp] : r * c2;   // EOS-0 store, ppm.cu:139
-        rv.f(2)[js] = hu[off + jp];
-        rv.f(3)[js] = hv[off + jp];
-        rv.f(4)[js] = (P.ndim == 3) ? hw[off + jp] : 0.0;
-      }
-      *rv.rot(0) = rot_v[rk]; *rv.rot(1) = res_v[rk];
-      *rv.rj(0) = rot_j[rk]; *rv.rj(1) = inc_j[rk];
-    }
+  pgk::pack_dump(run->T, D, P.ndim, run->fp32, run->p0_live ? 1 : 0, stage, s);
+  cudaError_t ce = cudaGetLastError();
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(rings, stage, bytes, cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+  cudaFree(stage);
+  if (ce != cudaSuccess) return fail(run, PG_ERR_CUDA, std::string("dump download: ") + cudaGetErrorString(ce));
+  run->launches += 1;
   return PG_OK;
 }
 

@@ -367,6 +367,12 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
   const int nphi = T.nphi, nrg = T.nrg, nk = T.nk;
   const int row = i + NPAD;
   const bool last = (l == T.cz.loop - 1);
+  // with ctl.fuse (a 3D step whose polar chunks are never idle) the store
+  // also damps and takes the next get_dt's CFL rate, as the separate damping
+  // and CFL kernels would on the stored state (k_damp_clk, k_cfl_clk)
+  __shared__ unsigned long long s_rate;
+  __shared__ int s_bad;
+  if (ctl.fuse && threadIdx.x == 0) { s_rate = 0ull; s_bad = 0; }
   if (last && T.cz.stuck) {
     int k = REAL * l + n;
     if (store && n < REAL && k < nk) {
@@ -461,12 +467,44 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
   if (store && n >= NPAD && n < lim - NPAD) {
     // the polar sweep is the last of a 3D step: the FARGO integer shift of
     // each layer (rotate_rings, ppm.cu:309-322) is applied at this store
-    int inc = ctl.shift ? T.inc_j[kr * nrg + row] : 0;
-    size_t o = (size_t)(kr * nrg + row) * nphi + wrapm(j0 + inc, nphi);
-    P.ro[o] = S.r[n];
-    P.wo[o] = S.u[n];
-    P.uo[o] = S.v[n];
-    P.vo[o] = S.w[n] / rad_cyl;
+    const int rkk = kr * nrg + row;
+    int inc = ctl.shift ? T.inc_j[rkk] : 0;
+    const int jo = wrapm(j0 + inc, nphi);
+    size_t o = (size_t)rkk * nphi + jo;
+    double r = S.r[n], vr = S.v[n], vp = S.w[n] / rad_cyl, vt = S.u[n];
+    if (ctl.fuse) {
+      const double g = T.damp_g[rkk];
+      if (g > 0.0) {
+        const double f = g * (st.dt * T.damp_pw[rkk]);
+        r += f * (T.val_r[rkk] - r);
+        vr += f * (T.val_u[rkk] - vr);
+        vp += f * (T.val_v[rkk] - vp);
+        vt += f * (-vt);
+      }
+      if (!ctl.nocfl) {
+        const double rad_c = T.radc[rkk];
+        const int js = wrapm(jo - (T.rot_j[rkk] + inc), nphi);
+        double p = r * T.cs2[rkk];
+        double cs = sqrt(ph.gam * p / r);
+        double t0 = (fabs(vr) + cs) / T.rdx[row];
+        double t1 = (fabs(vp - T.rot_v[rkk] - st.frrot_next * rad_c) + cs) / (T.dy[js] * rad_c);
+        double t2 = (fabs(vt) + cs) / (T.dz[kr + NPAD] * rad);
+        double rt = max3(t0, t1, t2);
+        if (rt > 0.0 || rt != rt) atomicMax(&s_rate, dbits(rt));
+      }
+      if (!(r > 0.0) || !isfinite(r) || !isfinite(vr) || !isfinite(vp)) s_bad = 1;
+    }
+    P.ro[o] = r;
+    P.wo[o] = vt;
+    P.uo[o] = vr;
+    P.vo[o] = vp;
+  }
+  if (ctl.fuse) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (s_rate) atomicMax(&ctl.clk->cfl_bits, s_rate);
+      if (s_bad) atomicExch(&ctl.clk->status, 3);
+    }
   }
 }
 

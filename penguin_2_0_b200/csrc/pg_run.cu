@@ -892,14 +892,20 @@ static int enqueue_step(pg_run *run, bool first_p0) {
     if (tm && ev_pair(run, 1, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     pgk::sweep_y(run->T, planes_fwd(run, 1 - a, nullptr), run->ph, c, 3, s); n += ny(run);
     if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
-    // 3D: the polar sweep applies the FARGO shift; damping and CFL follow it
+    // 3D: the polar sweep applies the FARGO shift; damping and the CFL rate
+    // are fused into its store when its chunks are never idle
     if (tm && ev_pair(run, 2, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     c.shift = 1;
+    const bool fuse_z = !run->T.cz.stuck;
+    c.fuse = fuse_z;
+    c.nocfl = moving;
     pgk::sweep_z(run->T, planes_fwd(run, a, nullptr), run->ph, c, P.ntop, s); n += nz(run);
     if (tm && ev_close(run, e_k)) return fail(run, PG_ERR_CUDA, "event record");
     double **cp = run->planes[1 - a];
-    pgk::damp_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->clk, s); n++;
-    if (!moving) { pgk::cfl_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->ph, run->clk, s); n++; }
+    if (!fuse_z) {
+      pgk::damp_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->clk, s); n++;
+      if (!moving) { pgk::cfl_clk(run->T, cp[0], cp[1], cp[2], cp[3], run->ph, run->clk, s); n++; }
+    }
     run->cur = 1 - a;
   }
   if (moving) {

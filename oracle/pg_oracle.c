@@ -62,7 +62,7 @@ static double G_vis_nu;
 
 static void set_globals(const pg_params *p) {
   G = *p;
-  G_vis_nu = p->ss_alpha * p->sc_h * p->sc_h;        /* global.h:216 */
+  G_vis_nu = p->ss_alpha * p->sc_h * p->sc_h;        /* global.h:36 */
 }
 
 static double cmin(double a, double b) { return fmin(a, b); }
@@ -302,7 +302,7 @@ static void blk_poison(oblk *B) {
   for (int c = 0; c < 5; c++) for (int n = 0; n < NPAD; n++) B->rg[c][n] = nan;
 }
 
-/* paraset parabola.cu:236-274 */
+/* paraset parabola.cu:138-176 */
 static void paraset(oblk *B, int nmin, int nmax, const double *dx, double *a, double *ai, double *b) {
   FOR_ACT(n) {
     B->par[n].c0 = B->par[n].c1 = B->par[n].c2 = B->par[n].c3 = B->par[n].c4 = NAN;
@@ -334,7 +334,7 @@ static void paraset(oblk *B, int nmin, int nmax, const double *dx, double *a, do
   }
 }
 
-/* parabola parabola.cu:168-231 (CW84 eq 1.5-1.8, 1.10) */
+/* parabola parabola.cu:70-133 (CW84 eq 1.5-1.8, 1.10) */
 static void parabola(oblk *B, int nmin, int nmax, const double *flat, const double *val,
                      double *al, double *da, double *a6) {
   FOR_ACT(n) {
@@ -453,7 +453,7 @@ static void states(oblk *B, int nmax, double hdt, int axis, const obody *pl,
   }
 }
 
-/* riemann riemann.cu:76-188, isothermal branch (EOS 0, 119-126) */
+/* riemann riemann.cu:3-115, isothermal branch (EOS 0, 45-53) */
 static void riemann(oblk *B, int nmax, double *umid, double *pmid) {
   FOR_ACT(n) {
     if (n >= 3 && n < nmax - 2) {
@@ -1117,7 +1117,7 @@ double orc_get_dt(orc_run *R, double dt, double FrRot) {
   return dt;
 }
 
-/* bin_reduc_sum reduction.cu:120-142 on a 1024 list */
+/* bin_reduc_sum reduction.cu:123-142 on a 1024 list */
 static double tree1024(double *list) {
   for (int len = 1024; len > 1; len /= 2) {
     int half = len / 2;

@@ -179,7 +179,7 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   }
   __syncthreads();
 
-  // ---- riemann riemann.cu:76-188, isothermal (119-126) ----
+  // ---- riemann riemann.cu:3-115, isothermal (45-53) ----
   if (n >= 3 && n < nmax - 2) {
     double t1 = 0.5 * (sqrt(spl / srl) + sqrt(spr / srr));
     double t2 = -0.5 * (sur - sul) / t1;
@@ -263,7 +263,7 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   } else if (AXIS == 1) {
     lvol = (xa - xa0n) * c.rad;
   } else {
-    // remap.cu:221, cancellation-free form of (cos(xa0) - cos(xa)) * rad
+    // remap.cu:53, cancellation-free form of (cos(xa0) - cos(xa)) * rad
     double d = xa - xa0n;
     lvol = 2.0 * sin(xa0n + 0.5 * d) * sin(0.5 * d) * c.rad;
   }

@@ -47,7 +47,7 @@ double Profile::dP_s(double r, double pol) const {                              
   return (pres(r1, z1) - pres(r2, z2)) / (2.0 * dr);
 }
 double Profile::nu(double r) const {                                             // 149-152
-  double vis_nu = P.ss_alpha * P.sc_h * P.sc_h;                                  // global.h:216
+  double vis_nu = P.ss_alpha * P.sc_h * P.sc_h;                                  // global.h:36
   return vis_nu * std::pow(r, P.p_alpha);
 }
 double Profile::viscous_vr(double r) const {                                     // 154-160

@@ -793,7 +793,7 @@ __device__ __forceinline__ void reduce_body(const Tables &T, const RT *R, Body p
   __syncthreads();
   if (!is_last) return;
   __threadfence();
-  // lv2 (3D): round_reduc_sum over k per ring i, reduction.cu:75-100
+  // lv2 (3D): round_reduc_sum over k per ring i, reduction.cu:77-100
   const volatile double *part = ring_part;
   int nr = T.nr, nk = T.nk;
   // lv3: rings in chunks of 1024 (the reference supports iblk <= 1024)

@@ -13,7 +13,7 @@
 //    from a separate buffer, instead of one CTA walking the pencil with a
 //    6-cell carry (ppm.cu:43-157 carries pre-update values, so the result is
 //    the same Jacobi update);
-//  * the q = p/rho remap (remap.cu:291-300) is skipped: in EOS 0 the sweep
+//  * the q = p/rho remap (remap.cu:123-131) is skipped: in EOS 0 the sweep
 //    store overwrites p with rho*cs2 (ppm.cu:139);
 //  * in 2D the remap of the slot holding w is skipped (w stays exactly 0:
 //    the w slot of the radial sweep, the v slot of the azimuthal sweep) and
@@ -153,7 +153,7 @@ __device__ __forceinline__ double max3(double A, double B, double C) {   // simp
   else       { if (C > B) return C; else return B; }
 }
 
-// paraset parabola.cu:236-274 (non-uniform PPM interface coefficients)
+// paraset parabola.cu:138-176 (non-uniform PPM interface coefficients)
 __device__ __forceinline__ void paraset(int n, int nmin, int nmax, Par &par, const double *dx,
                                         double *a, double *ai, double *b) {
   double dx_n = 0.0, ain = 0.0, bi = 0.0, ci = 0.0, c = 0.0;
@@ -182,7 +182,7 @@ __device__ __forceinline__ void paraset(int n, int nmin, int nmax, Par &par, con
   __syncthreads();
 }
 
-// parabola parabola.cu:168-231 (CW84 eq 1.5-1.8, 1.10)
+// parabola parabola.cu:70-133 (CW84 eq 1.5-1.8, 1.10)
 __device__ __forceinline__ void parabola(int n, int nmin, int nmax, double flat, const double *val,
                                          double *al, double *da, double *a6, const Par &par) {
   double t1 = 0.0, a = 0.0, ar = 0.0, da_r = 0.0;

@@ -577,7 +577,7 @@ static void remap(oblk *B, int nmax, int axis, double *al, double *da, double *a
     } else {
       if (G.ngeomz == 0) lvol = xa - x0;
       else if (G.ngeomz == 5) {
-        double d = xa - x0;   /* remap.cu:221 without cancellation */
+        double d = xa - x0;   /* remap.cu:53 without cancellation */
         lvol = 2.0 * sin(x0 + 0.5 * d) * sin(0.5 * d) * B->rad[n];
       }
     }
@@ -1172,7 +1172,7 @@ double orc_reduce(orc_run *R, const pg_body *plb, double exclude, int mode) {
   double *d1 = d2;
   double *tmp1d = NULL;
   if (G.ndim == 3) {
-    /* output_lv2: round_reduc_sum over k (reduction.cu:75-100) */
+    /* output_lv2: round_reduc_sum over k (reduction.cu:77-100) */
     tmp1d = (double *)calloc(iblk, sizeof(double));
     double *rl = (double *)malloc(sizeof(double) * kblk);
     for (int i = 0; i < iblk; i++) {

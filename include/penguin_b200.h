@@ -102,9 +102,11 @@ int pg_default_params(pg_params *p);
  * 128x1024x32 spherical disk, 2 = 2D 1024x3072 disk.                       */
 int pg_config_params(int which, pg_params *p);
 
-/* Checks a parameter set; PG_ERR_PARAMS with a message for combinations the
- * reference does not implement (EOS != 0, bary_flag, ...) or whose sweep
- * chunking would read already-updated cells (jmax % 116 in 1..5).          */
+/* Checks a parameter set; PG_ERR_PARAMS with a message for combinations
+ * that are not implemented (EOS 2, which the reference marks buggy;
+ * bary_flag; EOS 1 on FP32 planes, ...) or whose sweep chunking would read
+ * already-updated cells (jmax % 116 in 1..5).  EOS 0 (isothermal) and EOS 1
+ * (isentropic, p = cs2 Sigma^gam / gam) run in 2D and 3D.                  */
 int pg_check_params(const pg_params *p);
 
 /* Size in bytes of one hydr_ring record of the dump layout

@@ -81,10 +81,17 @@ static double max3(double A, double B, double C) {
 /* ------------------------------------------------------------------------ */
 /* disk profile (disk_profile.cu)                                           */
 
-static double get_rho1(double r) { return pow(r, -G.p_alpha); }             /* 9-28 */
+static double get_rho1(double r) {                                         /* 9-28 */
+  double n = -G.p_alpha;
+  if (G.EOS != 0 && G.ndim == 3) n = -G.p_alpha * (2.0 / (G.gam + 1.0));
+  return pow(r, n);
+}
 static double get_cs2(double r) { return G.sc_h * G.sc_h * pow(r, -G.p_beta); } /* 39-42 */
 static double get_h(double r) { return sqrt(get_cs2(r) * r * r * r); }      /* 49-52 */
-static double get_P1(double r) { return get_cs2(r) * get_rho1(r); }         /* 54-61 */
+static double get_P1(double r) {                                           /* 54-61 */
+  if (G.EOS == 0) return get_cs2(r) * get_rho1(r);
+  return get_cs2(r) * pow(get_rho1(r), G.gam) / G.gam;
+}
 static double get_dP_dr1(double r) {                                       /* 63-68 */
   double p1 = get_P1(r + 1.27245e-8);
   double p2 = get_P1(r - 1.27245e-8);
@@ -95,8 +102,26 @@ static double get_verfac(double r, double z) {                              /* 7
   double rr = sqrt(r * r + z * z);
   return exp((1.0 / rr - 1.0 / r) / cs2);
 }
-static double get_rho2(double r, double z) { return get_rho1(r) * get_verfac(r, z); } /* 86-89 */
-static double get_P2(double r, double z) { return get_cs2(r) * get_rho2(r, z); }     /* 112-115 */
+static double get_rho2(double r, double z) {                               /* 86-103 */
+  double gamm, h, z_0, base;
+  if (G.EOS == 0) return get_rho1(r) * get_verfac(r, z);
+  gamm = G.gam - 1.0;
+  h = sqrt(get_cs2(r) * r * r * r);
+  z_0 = sqrt(2.0 * h * h * pow(r, -G.p_alpha * (2.0 / (G.gam + 1.0)) * gamm) / gamm);
+  if (z < z_0)
+    return pow(pow(get_rho1(r), gamm) - (gamm / (r * get_cs2(r))) * (1.0 - r / sqrt(r * r + z * z)), 1.0 / gamm);
+  base = pow(pow(get_rho1(r), gamm) - (gamm / (r * get_cs2(r))) * (1.0 - r / sqrt(r * r + z_0 * z_0)), 1.0 / gamm);
+  return pow(10.0, log10(base) - 6.0 * (z - z_0) / h);
+}
+static double get_P2(double r, double z) {                                 /* 112-118 */
+  if (G.EOS == 0) return get_cs2(r) * get_rho2(r, z);
+  return get_cs2(r) * pow(get_rho2(r, z), G.gam) / G.gam;
+}
+/* the sweep store's pressure (ppm.cu:138-143): EOS 0 r cs2, EOS 1 cs2 r^gam / gam */
+static double store_p(double r, double cs2) {
+  if (G.EOS == 0) return r * cs2;
+  return cs2 * pow(r, G.gam) / G.gam;
+}
 static double get_dP_s(double r, double pol) {                              /* 128-138 */
   double dr = 1.27e-7;
   double sinpol = sin(pol);
@@ -453,12 +478,48 @@ static void states(oblk *B, int nmax, double hdt, int axis, const obody *pl,
   }
 }
 
-/* riemann riemann.cu:3-115, isothermal branch (EOS 0, 45-53) */
+/* riemann riemann.cu:75-111, the EOS 1 branch: van Leer's Newton iteration
+ * on the Lagrangian sound speeds (at most 10 passes, tolerance 1e-8) */
+static void riemann_newton(double pl, double rl, double ul, double pr, double rr, double ur,
+                           double *umid, double *pmid) {
+  const double gamfac2 = G.gam + 1.0, gamfac1 = gamfac2 / G.gam / 2.0;
+  double cs_l = sqrt(G.gam * pl * rl), cs_r = sqrt(G.gam * pr * rr);
+  double pm, t1 = 0.0, t2 = 0.0, en_l, en_r, dum, uml, umr;
+  int l;
+  rl = 1.0 / rl;
+  rr = 1.0 / rr;
+  pm = pr - pl - cs_r * (ur - ul);
+  pm = pl + pm * cs_l / (cs_l + cs_r);
+  pm = cmax(k_smallp, pm);
+  for (l = 0; l < 10; l++) {
+    dum = pm;
+    t1 = 1.0 + gamfac1 * (pm - pl) / pl;
+    t2 = 1.0 + gamfac1 * (pm - pr) / pr;
+    t1 = cs_l * sqrt(t1);
+    t2 = cs_r * sqrt(t2);
+    en_l = 4.0 * rl * t1 * t1;
+    en_r = 4.0 * rr * t2 * t2;
+    en_l = -en_l * t1 / (en_l - gamfac2 * (pm - pl));
+    en_r = en_r * t2 / (en_r - gamfac2 * (pm - pr));
+    uml = ul - (pm - pl) / t1;
+    umr = ur + (pm - pr) / t2;
+    pm = pm + (umr - uml) * (en_r * en_l) / (en_r - en_l);
+    pm = cmax(k_smallp, pm);
+    if (fabs(pm - dum) / pm < 1.0e-8) break;
+  }
+  uml = ul - (pm - pl) / t1;
+  umr = ur + (pm - pr) / t2;
+  *umid = 0.5 * (uml + umr);
+  *pmid = cmax(k_smallp, pm);
+}
+
+/* riemann riemann.cu:3-115: isothermal (EOS 0, 45-53) or isentropic (EOS 1) */
 static void riemann(oblk *B, int nmax, double *umid, double *pmid) {
   FOR_ACT(n) {
     if (n >= 3 && n < nmax - 2) {
       double pl = B->S[n].pl, rl = B->S[n].rl, ul = B->S[n].ul;
       double pr = B->S[n].pr, rr = B->S[n].rr, ur = B->S[n].ur;
+      if (G.EOS == 1) { riemann_newton(pl, rl, ul, pr, rr, ur, &umid[n], &pmid[n]); continue; }
       double t1 = 0.5 * (sqrt(pl / rl) + sqrt(pr / rr));
       double t2 = -0.5 * (ur - ul) / t1;
       double pm = sqrt(pl * pr) * exp(t2);
@@ -538,7 +599,7 @@ static void evolve(oblk *B, int nmax, double dt, int axis, double FrRot, const o
   }
   FOR_ACT(n) {
     if (n >= 3 && n < nmax - 3) {
-      B->q[n] = B->p[n] / B->r[n];
+      B->q[n] = (G.EOS == 0) ? B->p[n] / B->r[n] : B->p[n] / pow(B->r[n], G.gam);   /* evolve.cu:131-135 */
       B->r[n] = cmax(B->r[n] * (B->dvol0[n] / B->dvol[n]), k_smallr);
       double dum = B->u[n];
       double delx = 0.5 * dt * (B->fto1[n] + B->fto2[n]);
@@ -560,8 +621,8 @@ static void get_flux(oblk *B, int nmax, double *flux, const double *al, const do
   FOR_ACT(n) out[n] = flux[n] - flux[n + 1];
 }
 
-/* remap remap.cu:14-226 (EOS 0: the q remap sets p, which the sweep store
- * later overwrites with r*cs2; it is kept here as in the reference) */
+/* remap remap.cu:14-226 (the q remap sets p, which the sweep store later
+ * overwrites by the EOS relation; it is kept here as in the reference) */
 static void remap(oblk *B, int nmax, int axis, double *al, double *da, double *a6) {
   double fluxn[ARR];
   paraset(B, 3, nmax - 3, B->dx, al, da, a6);
@@ -626,7 +687,7 @@ static void remap(oblk *B, int nmax, int axis, double *al, double *da, double *a
   FOR_ACT(n) {
     if (n >= 6 && n < nmax - 6) {
       B->q[n] = (B->q[n] * B->mm[n] + fluxn[n]) * B->invm[n];
-      B->p[n] = cmax(k_smallp, B->r[n] * B->q[n]);
+      B->p[n] = cmax(k_smallp, (G.EOS == 0) ? B->r[n] * B->q[n] : pow(B->r[n], G.gam) * B->q[n]);  /* remap.cu:123-142 */
     }
   }
 }
@@ -807,7 +868,7 @@ static void sweepx_block(orc_run *R, oblk *B, int j0, int k_ring, double dt, con
         oring *c = cur[i];
         int j = jj[i];
         c->r[j] = B->r[i];
-        c->p[j] = B->r[i] * get_cs2(radc[i]);
+        c->p[j] = store_p(B->r[i], get_cs2(radc[i]));
         c->u[j] = B->u[i];
         if (G.ngeomy > 2) c->v[j] = B->v[i] / radc[i];
         else c->v[j] = B->v[i];
@@ -881,7 +942,7 @@ static void sweepy_block(orc_run *R, oblk *B, int nring, double dt, const obody 
       if (i >= NPAD && i < lim - NPAD) {
         int j = jj[i];
         c->r[j] = B->r[i];
-        c->p[j] = B->r[i] * get_cs2(rad_cyl);
+        c->p[j] = store_p(B->r[i], get_cs2(rad_cyl));
         c->u[j] = B->w[i];
         c->v[j] = B->u[i];
         c->w[j] = B->v[i];
@@ -996,7 +1057,7 @@ static void sweepz_block(orc_run *R, oblk *B, int i_rad, int j0, double dt, cons
         oring *c = cur[i];
         int j = jj[i];
         c->r[j] = B->r[i];
-        c->p[j] = B->r[i] * get_cs2(radc[i]);
+        c->p[j] = store_p(B->r[i], get_cs2(radc[i]));
         c->w[j] = B->u[i];
         c->u[j] = B->v[i];
         c->v[j] = B->w[i] / radc[i];
@@ -1456,8 +1517,8 @@ int orc_save(const orc_run *R, void *buf, size_t bytes) {
 
 /* ------------------------------------------------------------------------ */
 /* wave damping: kill_wave.cu:19-40 restated for zones r < kill_rin and
- * r > kill_rout, relaxing toward the axisymmetric profile; p re-derived as
- * Sigma*cs2 so the EOS-0 invariant p == r*cs2 of the sweep store holds.    */
+ * r > kill_rout, relaxing toward the axisymmetric profile; p re-derived by
+ * the sweep store's relation (Sigma cs2, or cs2 Sigma^gam / gam in EOS 1). */
 void orc_damp(orc_run *R, double dt) {
   set_globals(&R->P);
   if (!(G.kill_rin > 0.0) && !(G.kill_rout > 0.0)) return;
@@ -1477,7 +1538,7 @@ void orc_damp(orc_run *R, double dt) {
       c->u[j] += f * (v0->u - c->u[j]);
       c->v[j] += f * (v0->v - c->v[j]);
       c->w[j] += f * (-c->w[j]);
-      c->p[j] = c->r[j] * cs2;
+      c->p[j] = store_p(c->r[j], cs2);
     }
   }
 }

@@ -46,7 +46,8 @@ sdp *zxa, *zxc, *zdx, *zya, *zyc, *zdy, *zza, *zzc, *zdz;
 #include "init.cpp"
 
 // Damping toward the axisymmetric profile val[] (the rule used by the
-// oracle and by the CUDA path): f = dt r^-1.5 (distance into zone / width).
+// oracle and by the CUDA path): f = dt r^-1.5 (distance into zone / width);
+// p is then re-derived by the sweep store's EOS relation.
 __global__ void harness_damp(hydr_ring *rings, SymDisk *val, sdp dt, int nring)
 {
   int n = blockIdx.x;
@@ -65,7 +66,11 @@ __global__ void harness_damp(hydr_ring *rings, SymDisk *val, sdp dt, int nring)
     rings[n].u[j] += f * (val[idx].u - rings[n].u[j]);
     rings[n].v[j] += f * (val[idx].v - rings[n].v[j]);
     rings[n].w[j] += f * (-rings[n].w[j]);
+#if EOS == 1
+    rings[n].p[j] = cs2 * pow(rings[n].r[j], gam) / gam;   // the sweep store's p, ppm.cu:140-141
+#else
     rings[n].p[j] = rings[n].r[j] * cs2;
+#endif
   }
 }
 

@@ -9,8 +9,9 @@
 //     pencil chunks of every member; CTA b takes tiles b, b + grid, ...),
 //     poststep, mass and torque reductions (one CTA per ring of every member)
 //     and the history record.
-//   * 3D members and members with a moving planet (plnt_flag 2) take their
-//     own launch sequence (the per-run fused step) in the same stream order.
+//   * 3D members, members with a moving planet (plnt_flag 2) and isentropic
+//     members (EOS 1) take their own launch sequence (the per-run fused
+//     step) in the same stream order; the queue kernels are isothermal 2D.
 // The step sequence of `chunk` steps is captured once as a CUDA graph and
 // replayed; membership changes rebuild the descriptors and the graph.
 #include <cuda_runtime.h>
@@ -56,7 +57,7 @@ struct pg_batch {
   std::string err;
   std::vector<pg_run *> runs;      // in the order added
   Group g[2];                      // 2D members: FP64, FP32
-  std::vector<pg_run *> solo;      // 3D members
+  std::vector<pg_run *> solo;      // members with their own step sequence
   bool dirty = true;
   cudaGraphExec_t gexec = nullptr;
   int gsteps = 0;
@@ -100,7 +101,7 @@ static int rebuild(pg_batch *b) {
   for (pg_run *r : b->runs) {
     pgi::RunShape sh;
     pgi::run_shape(r, &sh);
-    if (sh.ndim == 3 || sh.moving) b->solo.push_back(r);
+    if (sh.ndim == 3 || sh.moving || sh.eos) b->solo.push_back(r);
     else b->g[sh.fp32].members.push_back(r);
   }
   for (auto &g : b->g) {

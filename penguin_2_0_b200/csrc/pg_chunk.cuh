@@ -101,7 +101,7 @@ __device__ __forceinline__ double centre_force(int n, double dt, double rad, dou
 // The ppmlr chain for one chunk.  All threads of the CTA call it (it has
 // barriers); cells n >= nmax take no part in any phase.  On return r, u, v
 // (and w when THREED) hold the Lagrange-remapped values for 6 <= n < nmax-6.
-template <int AXIS, bool SPH, bool THREED, class SHM>
+template <int AXIS, bool SPH, bool THREED, int EOS = 0, class SHM>
 __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, double FrRot,
                                           const CellIn &c, const Body &pl, const Phys &ph) {
   const bool act = n < nmax;
@@ -179,13 +179,20 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   }
   __syncthreads();
 
-  // ---- riemann riemann.cu:3-115, isothermal (45-53) ----
+  // ---- riemann riemann.cu:3-115, isothermal (45-53) or isentropic (75-111) ----
   if (n >= 3 && n < nmax - 2) {
-    double t1 = 0.5 * (sqrt(spl / srl) + sqrt(spr / srr));
-    double t2 = -0.5 * (sur - sul) / t1;
-    double pm = sqrt(spl * spr) * exp(t2);
-    S.umid[n] = sul - t1 * log(pm / spl);
-    S.pmid[n] = fmax(kSmallp, pm);
+    if (EOS == 0) {
+      double t1 = 0.5 * (sqrt(spl / srl) + sqrt(spr / srr));
+      double t2 = -0.5 * (sur - sul) / t1;
+      double pm = sqrt(spl * spr) * exp(t2);
+      S.umid[n] = sul - t1 * log(pm / spl);
+      S.pmid[n] = fmax(kSmallp, pm);
+    } else {
+      double um, pm;
+      riemann_isentropic(spl, srl, sul, spr, srr, sur, ph, um, pm);
+      S.umid[n] = um;
+      S.pmid[n] = pm;
+    }
   }
   __syncthreads();
 

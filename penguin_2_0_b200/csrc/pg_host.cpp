@@ -23,10 +23,17 @@ const double kJupiterMass = 0.001;
 const double kMMSN = 0.00019126835;
 
 // ---- disk profile (disk_profile.cu) --------------------------------------
-double Profile::rho(double r) const { return std::pow(r, -P.p_alpha); }          // 9-28
+double Profile::rho(double r) const {                                           // 9-28
+  // the 3D isentropic disk's midplane slope is p_alpha 2/(gam + 1)
+  double n = (P.EOS != 0 && P.ndim == 3) ? -P.p_alpha * (2.0 / (P.gam + 1.0)) : -P.p_alpha;
+  return std::pow(r, n);
+}
 double Profile::cs2(double r) const { return P.sc_h * P.sc_h * std::pow(r, -P.p_beta); }  // 39-42
 double Profile::h(double r) const { return std::sqrt(cs2(r) * r * r * r); }      // 49-52
-double Profile::pres(double r) const { return cs2(r) * rho(r); }                 // 54-61
+double Profile::pres(double r) const {                                          // 54-61
+  if (P.EOS == 0) return cs2(r) * rho(r);
+  return cs2(r) * std::pow(rho(r), P.gam) / P.gam;
+}
 double Profile::dP_dr(double r) const {                                          // 63-68
   double p1 = pres(r + 1.27245e-8);
   double p2 = pres(r - 1.27245e-8);
@@ -37,8 +44,21 @@ double Profile::verfac(double r, double z) const {                              
   double rr = std::sqrt(r * r + z * z);
   return std::exp((1.0 / rr - 1.0 / r) / c);
 }
-double Profile::rho(double r, double z) const { return rho(r) * verfac(r, z); }  // 86-89
-double Profile::pres(double r, double z) const { return cs2(r) * rho(r, z); }    // 112-115
+double Profile::rho(double r, double z) const {                                 // 86-103
+  if (P.EOS == 0) return rho(r) * verfac(r, z);
+  // isentropic: the polytrope rho^(gam-1) = rho_mid^(gam-1) - (gam-1)/(r cs2)
+  // (1 - r/sqrt(r^2 + z^2)), continued above z_0 by a decade per h/6
+  const double gm = P.gam - 1.0;
+  double h = std::sqrt(cs2(r) * r * r * r);
+  double z0 = std::sqrt(2.0 * h * h * std::pow(r, -P.p_alpha * (2.0 / (P.gam + 1.0)) * gm) / gm);
+  if (z < z0) return std::pow(std::pow(rho(r), gm) - (gm / (r * cs2(r))) * (1.0 - r / std::sqrt(r * r + z * z)), 1.0 / gm);
+  double top = std::pow(std::pow(rho(r), gm) - (gm / (r * cs2(r))) * (1.0 - r / std::sqrt(r * r + z0 * z0)), 1.0 / gm);
+  return std::pow(10.0, std::log10(top) - 6.0 * (z - z0) / h);
+}
+double Profile::pres(double r, double z) const {                                // 112-118
+  if (P.EOS == 0) return cs2(r) * rho(r, z);
+  return cs2(r) * std::pow(rho(r, z), P.gam) / P.gam;
+}
 double Profile::dP_s(double r, double pol) const {                               // 128-138
   double dr = 1.27e-7;
   double sp = std::sin(pol), cp = std::cos(pol);
@@ -274,7 +294,15 @@ int check_params(const pg_params *p, std::string &why) {
   if (p->imax < 1 || p->jmax < 1 || p->kmax < 1) { why = "grid sizes must be positive"; return PG_ERR_PARAMS; }
   if (p->ndim == 2 && p->kmax != 1) { why = "2D problem needs kmax == 1 (main.cu:130)"; return PG_ERR_PARAMS; }
   if (p->ndim == 3 && p->kmax == 1) { why = "3D problem needs kmax > 1 (main.cu:134)"; return PG_ERR_PARAMS; }
-  if (p->EOS != 0) { why = "only the isothermal EOS 0 is implemented (global.h:18 marks 2 buggy)"; return PG_ERR_PARAMS; }
+  if (p->EOS == 2) {
+    why = "EOS 2 (energy equation) is not implemented: the reference marks it buggy (global.h:18)"; return PG_ERR_PARAMS;
+  }
+  if (p->EOS != 0 && p->EOS != 1) { why = "EOS must be 0 (isothermal) or 1 (isentropic)"; return PG_ERR_PARAMS; }
+  if (!(p->gam >= 1.0)) { why = "gam must be >= 1"; return PG_ERR_PARAMS; }
+  if (p->EOS == 1 && p->ndim == 3 && !(p->gam > 1.0)) {
+    why = "3D EOS 1 needs gam > 1 (the vertical polytrope divides by gam - 1)"; return PG_ERR_PARAMS;
+  }
+  if (p->EOS == 1 && p->precision != 0) { why = "the FP32 planes implement EOS 0 only"; return PG_ERR_PARAMS; }
   if (p->bary_flag) { why = "barycentric frame (bary_flag) is not implemented"; return PG_ERR_PARAMS; }
   if (p->kill_flag != 0) { why = "kill_flag is not implemented in the reference; use kill_rin/kill_rout"; return PG_ERR_PARAMS; }
   if (p->plnt_flag < 0 || p->plnt_flag > 2) { why = "plnt_flag must be 0, 1 or 2"; return PG_ERR_PARAMS; }
@@ -306,7 +334,8 @@ int check_params(const pg_params *p, std::string &why) {
 // ---- seeded initial condition ------------------------------------------------
 // init_grid + init_den + init_speed + init_cells (init.cpp:3-249) with
 // Sigma = val.r * (1 + noise_amp*(2U-1)), U = splitmix64(seed, ring*jmax+j),
-// v_r = 0, p = Sigma*cs2(r_cyl) (the EOS-0 store of ppm.cu:139), rot_j = 0,
+// v_r = 0, p = Sigma*cs2(r_cyl) or cs2 Sigma^gam/gam (the sweep store of
+// ppm.cu:138-143 for EOS 0 / 1), rot_j = 0,
 // rot_v = val.v - FrRot*xc (the FARGO_flag 1 value of orbital_advection.cu:22).
 int build_ic(const pg_params *p, void *buf, size_t bytes, std::string &why) {
   int st = check_params(p, why);
@@ -347,7 +376,7 @@ int build_ic(const pg_params *p, void *buf, size_t bytes, std::string &why) {
         double U = ic_uniform(P.seed, (uint64_t)m * P.jmax + j);
         double sig = v.r * (1.0 + P.noise_amp * (2.0 * U - 1.0));
         rv.f(0)[j] = sig;
-        rv.f(1)[j] = sig * c2;
+        rv.f(1)[j] = (P.EOS == 0) ? sig * c2 : c2 * std::pow(sig, P.gam) / P.gam;
         rv.f(2)[j] = 0.0;
         rv.f(3)[j] = v.v;
         rv.f(4)[j] = 0.0;
@@ -369,9 +398,13 @@ std::string label(const pg_params &P) {
   else if (P.plnt_flag == 1) s += "_p" + itos((int)std::round(P.M_p / 0.000003)) + "_s" + itos((int)std::round(100.0 * P.rs_fac));
   s += "_i" + itos((int)(P.xmin * 100.0)) + "_o" + itos((int)(P.xmax * 100.0));
   if (P.visc_flag == 1) s += "_a" + itos((int)std::round(P.ss_alpha * 10000.0));
-  if (P.p_alpha + 0.5 * P.p_beta - 1.5 == 1.5) s += "_flatvor";
-  if (P.p_beta == 0.0) s += "_iso";
-  else s += "_b" + itos((int)(P.p_beta * 10.0));
+  if (P.EOS == 1) {
+    s += "_g" + itos((int)std::round(P.gam * 10.0));
+  } else {
+    if (P.p_alpha + 0.5 * P.p_beta - 1.5 == 1.5) s += "_flatvor";
+    if (P.p_beta == 0.0) s += "_iso";
+    else s += "_b" + itos((int)(P.p_beta * 10.0));
+  }
   if (P.FrRot_flag == 1) s += "_rot";
   if (P.FARGO_flag == 1) s += "_fargo";
   return s;

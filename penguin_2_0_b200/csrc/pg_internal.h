@@ -12,6 +12,7 @@ namespace pgi {
 struct RunShape {
   int dev, ndim, fp32, loaded, clock_ready, p0_live;
   int moving;              // plnt_flag 2: the planet feels the disk (own step sequence)
+  int eos;                 // EOS 1: isentropic sweeps (own step sequence)
   int nr, nphi, nk;
   int tiles_x, tiles_y;    // 2D pencil chunks of the radial and azimuthal sweeps
   int tiles_xs;            // radial last chunks of at most 64 cells, 4 columns per tile

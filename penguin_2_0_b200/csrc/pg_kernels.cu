@@ -74,7 +74,7 @@ __device__ __forceinline__ bool load_step(const SweepCtl &c, StepIn &s) {
 // radial sweep
 // One radial pencil chunk: column j0, chunk l, polar layer k.  The body is
 // shared by the per-run kernel and the batched kernels of pg_batch.cu.
-template <bool SPH, bool THREED, int NT>
+template <bool SPH, bool THREED, int NT, int EOS = 0>
 __device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, int n, bool store, const Tables &T, const Planes &P,
                                              const Phys &ph, const SweepCtl &ctl, const StepIn &st, int j0, int l,
                                              int k) {
@@ -114,12 +114,12 @@ __device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, int n, bool store
     if (THREED) S.w[n] = P.w[idx] * c.rad;
     else S.w[n] = 0.0;
     bool ghost = (row < NPAD) || (row >= T.nr + NPAD);
-    S.p[n] = ghost ? T.gp[rk] : (P.p0 ? P.p0[idx] : r * T.cs2[rk]);
+    S.p[n] = ghost ? T.gp[rk] : (P.p0 ? P.p0[idx] : eos_p<EOS>(r, T.cs2[rk], ph));
   } else {
     c.rad = 1.0; c.azi = 0.0; c.pol = 0.0; c.dvol0 = 1.0; c.vrot = 0.0; c.sinpol = 0.0;
   }
   __syncthreads();
-  ppm_chunk<0, SPH, THREED>(S, n, lim, st.dt, st.frrot, c, st.pl, ph);
+  ppm_chunk<0, SPH, THREED, EOS>(S, n, lim, st.dt, st.frrot, c, st.pl, ph);
   // device_viscosity_r viscosity.cu:370-421 (nu*rho scratch in dx0)
   if (ph.visc) {
     const double R = rad_cyl;
@@ -163,12 +163,12 @@ __device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, int n, bool store
   }
 }
 
-template <bool SPH, bool THREED, int NT, int MINB>
+template <bool SPH, bool THREED, int NT, int MINB, int EOS = 0>
 __global__ void __launch_bounds__(NT, MINB) k_sweep_x(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
   __shared__ ChunkShmT<NT> S;
   StepIn st;
   if (!load_step(ctl, st)) return;
-  sweep_x_body<SPH, THREED, NT>(S, threadIdx.x, true, T, P, ph, ctl, st, blockIdx.x, blockIdx.y + l0, blockIdx.z);
+  sweep_x_body<SPH, THREED, NT, EOS>(S, threadIdx.x, true, T, P, ph, ctl, st, blockIdx.x, blockIdx.y + l0, blockIdx.z);
 }
 
 // The short last chunk of radial pencils (lim <= 64 cells): 4 adjacent
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(4 * PX_LIM, MINB) k_sweep_x_packed(Tables T, P
 // azimuthal sweep with the FARGO shift at the store and the fused epilogue
 // One azimuthal chunk: chunk l of ring i in polar layer k; FARGO shift at
 // the store and, with ctl.fuse, damping and the CFL rate in the epilogue.
-template <bool SPH, bool THREED, int NT>
+template <bool SPH, bool THREED, int NT, int EOS = 0>
 __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, const Tables &T, const Planes &P,
                                              const Phys &ph, const SweepCtl &ctl, const StepIn &st, int l, int i,
                                              int k) {
@@ -224,8 +224,8 @@ __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, cons
         v += dampf * (T.val_v[rk] - v);
         if (THREED) w += dampf * (-w);
       }
-      // dt_lv1 timestep.cu:36-57 on the stored state (p = r*cs2)
-      double p = r * T.cs2[rk];
+      // dt_lv1 timestep.cu:36-57 on the stored state (p by the EOS relation)
+      double p = eos_p<EOS>(r, T.cs2[rk], ph);
       double cs = sqrt(ph.gam * p / r);
       int js = wrapm(jo - (T.rot_j[rk] + inc), nphi);
       double widthy = T.dy[js] * rad_cyl;
@@ -278,13 +278,13 @@ __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, cons
       S.dx0[n] = T.dy[j0];
       double r = P.r[s];
       S.r[n] = r;
-      S.p[n] = r * T.cs2[rk];
+      S.p[n] = eos_p<EOS>(r, T.cs2[rk], ph);
       S.u[n] = P.v[s];
       S.v[n] = THREED ? P.w[s] : 0.0;
       S.w[n] = P.u[s];
     }
     __syncthreads();
-    ppm_chunk<1, SPH, THREED>(S, n, lim, st.dt, st.frrot, c, st.pl, ph);
+    ppm_chunk<1, SPH, THREED, EOS>(S, n, lim, st.dt, st.frrot, c, st.pl, ph);
     // device_viscosity_p viscosity.cu:423-472 with x = r_cyl * phi_face,
     // u -> w slot (v_r), v -> u slot (v_phi), w -> v slot (v_theta)
     if (ph.visc) {
@@ -338,13 +338,13 @@ __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, cons
   }
 }
 
-template <bool SPH, bool THREED, int NT, int MINB>
+template <bool SPH, bool THREED, int NT, int MINB, int EOS = 0>
 __global__ void __launch_bounds__(NT, MINB) k_sweep_y(Tables T, Planes P, Phys ph, SweepCtl ctl, int l0) {
   __shared__ ChunkShmT<NT> S;
   __shared__ double red[NT / 32];
   StepIn st;
   if (!load_step(ctl, st)) return;
-  sweep_y_body<SPH, THREED, NT>(S, red, T, P, ph, ctl, st, blockIdx.x + l0, blockIdx.y, blockIdx.z);
+  sweep_y_body<SPH, THREED, NT, EOS>(S, red, T, P, ph, ctl, st, blockIdx.x + l0, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_y(Tables T, Planes P, Phys p
 // One pencil chunk: ring i, column j0, chunk l; n is this thread's cell in
 // the chunk and `store` false computes without storing (padding pencils of
 // the packed kernel).
-template <int NT>
+template <int NT, int EOS = 0>
 __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store, const Tables &T, const Planes &P,
                                              const Phys &ph, const SweepCtl &ctl, const StepIn &st, int ntop,
                                              int i, int j0, int l) {
@@ -412,7 +412,7 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
       if (ntop == 0) {
         int rkm = km * nrg + row;
         size_t s = (size_t)rkm * nphi + j0;
-        r = P.r[s]; p = r * T.cs2[rkm]; u = P.u[s]; v = P.v[s]; w = -P.w[s];
+        r = P.r[s]; p = eos_p<EOS>(r, T.cs2[rkm], ph); u = P.u[s]; v = P.v[s]; w = -P.w[s];
         c.vrot = T.res_v[rkm] / T.radc[rkm];
       } else {
         const double *g = T.tg + ((size_t)(NPAD + (kr - nk)) * T.nr + i) * 4;
@@ -425,7 +425,7 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
       za = T.z[kz]; dz = T.dz[kz]; zc = T.zc[kz]; zvol = T.zvol[kz];
       rad_cyl = T.radc[rkk];
       idx = (size_t)rkk * nphi + j0;
-      r = P.r[idx]; p = r * T.cs2[rkk]; u = P.u[idx]; v = P.v[idx]; w = P.w[idx];
+      r = P.r[idx]; p = eos_p<EOS>(r, T.cs2[rkk], ph); u = P.u[idx]; v = P.v[idx]; w = P.w[idx];
       c.vrot = T.res_v[rkk] / rad_cyl;
     }
     c.pol = zc;
@@ -438,7 +438,7 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
     S.w[n] = v * rad_cyl;       // angular momentum about the axis
   }
   __syncthreads();
-  ppm_chunk<2, true, true>(S, n, lim, st.dt, st.frrot, c, st.pl, ph);
+  ppm_chunk<2, true, true, EOS>(S, n, lim, st.dt, st.frrot, c, st.pl, ph);
   if (ph.visc) {
     double rho = 0.0, nr = 0.0, ddu = 0.0, ddv = 0.0;
     if (act) {
@@ -484,7 +484,7 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
       if (!ctl.nocfl) {
         const double rad_c = T.radc[rkk];
         const int js = wrapm(jo - (T.rot_j[rkk] + inc), nphi);
-        double p = r * T.cs2[rkk];
+        double p = eos_p<EOS>(r, T.cs2[rkk], ph);
         double cs = sqrt(ph.gam * p / r);
         double t0 = (fabs(vr) + cs) / T.rdx[row];
         double t1 = (fabs(vp - T.rot_v[rkk] - st.frrot_next * rad_c) + cs) / (T.dy[js] * rad_c);
@@ -508,12 +508,12 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
   }
 }
 
-template <int NT, int MINB>
+template <int NT, int MINB, int EOS = 0>
 __global__ void __launch_bounds__(NT, MINB) k_sweep_z(Tables T, Planes P, Phys ph, SweepCtl ctl, int ntop, int l0) {
   __shared__ ChunkShmT<NT> S;
   StepIn st;
   if (!load_step(ctl, st)) return;
-  sweep_z_body<NT>(S, threadIdx.x, true, T, P, ph, ctl, st, ntop, blockIdx.x, blockIdx.y, blockIdx.z + l0);
+  sweep_z_body<NT, EOS>(S, threadIdx.x, true, T, P, ph, ctl, st, ntop, blockIdx.x, blockIdx.y, blockIdx.z + l0);
 }
 
 // Polar sweep of single-chunk pencils (nk <= PZ_LIM - 12, the usual 3D
@@ -584,7 +584,7 @@ __global__ void k_cfl(Tables T, const double *R, const double *U, const double *
     // physical column j holds storage index js = j - rot_j
     int js = wrapm(j - T.rot_j[rk], T.nphi);
     double r = R[base + j];
-    double p = P0 ? P0[base + j] : r * T.cs2[rk];
+    double p = P0 ? P0[base + j] : eos_p_rt(r, T.cs2[rk], ph);
     double cs = sqrt(ph.gam * p / r);
     double t0 = (fabs(U[base + j]) + cs) / T.rdx[row];
     double t1 = (fabs(V[base + j] - T.rot_v[rk] - frrot * rad_cyl) + cs) / (T.dy[js] * rad_cyl);
@@ -690,7 +690,7 @@ __global__ void k_cfl_clk(Tables T, const double *R, const double *U, const doub
   for (int j = threadIdx.x; j < T.nphi; j += blockDim.x) {
     int js = wrapm(j - rotn, T.nphi);
     double r = R[base + j];
-    double p = r * T.cs2[rk];
+    double p = eos_p_rt(r, T.cs2[rk], ph);
     double cs = sqrt(ph.gam * p / r);
     double t0 = (fabs(U[base + j]) + cs) / T.rdx[row];
     double t1 = (fabs(V[base + j] - T.rot_v[rk] - frrot * rad_cyl) + cs) / (T.dy[js] * rad_cyl);
@@ -1064,7 +1064,7 @@ __global__ void k_fill_ghost_rows(Tables T, const double *ghosts, DumpPlanes D, 
 }
 
 // whole ring records (72*nphi + 96 bytes) in the dump layout
-__global__ void k_pack_dump(Tables T, DumpPlanes D, int ndim, int fp32, int p0_live, unsigned char *out) {
+__global__ void k_pack_dump(Tables T, DumpPlanes D, Phys ph, int ndim, int fp32, int p0_live, unsigned char *out) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y, k = blockIdx.z;
   const int nphi = T.nphi, row = i + NPAD, rk = k * T.nrg + row, kz = k + NPAD;
   if (j >= nphi) return;
@@ -1084,7 +1084,7 @@ __global__ void k_pack_dump(Tables T, DumpPlanes D, int ndim, int fp32, int p0_l
     w = (ndim == 3) ? D.w[o] : 0.0;
   }
   f[j] = r;
-  f[nphi + j] = p0_live ? D.p0[o] : r * T.cs2[rk];   // EOS-0 store, ppm.cu:139
+  f[nphi + j] = p0_live ? D.p0[o] : eos_p_rt(r, T.cs2[rk], ph);   // the store's p, ppm.cu:138-143
   f[2 * nphi + j] = u;
   f[3 * nphi + j] = v;
   f[4 * nphi + j] = w;
@@ -1279,85 +1279,115 @@ static inline int cta_for(int lim) { return lim <= 32 ? 32 : (lim <= 64 ? 64 : 1
 // Occupancy variant of the 128-thread sweeps: MINB 1 lets the compiler keep
 // ~76 registers (6 CTAs per SM), MINB 8 caps them at 64 (8 CTAs per SM, a
 // few spilled values).  Chosen per run (pg_run's tuning, PG_SWEEP_OCC).
-#define PG_LAUNCH_X(SPHV, TD, NTV, grid, l0)                                                   \
-  do {                                                                                          \
-    if ((NTV) == 128 && occ8) k_sweep_x<SPHV, TD, 128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, l0); \
-    else if ((NTV) == 128) k_sweep_x<SPHV, TD, 128, 1><<<grid, 128, 0, s>>>(T, P, ph, c, l0);  \
-    else if ((NTV) == 64) k_sweep_x<SPHV, TD, 64, 1><<<grid, 64, 0, s>>>(T, P, ph, c, l0);     \
-    else k_sweep_x<SPHV, TD, 32, 1><<<grid, 32, 0, s>>>(T, P, ph, c, l0);                      \
-  } while (0)
-#define PG_LAUNCH_Y(SPHV, TD, NTV, grid, l0)                                                   \
-  do {                                                                                          \
-    if ((NTV) == 128 && occ8) k_sweep_y<SPHV, TD, 128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, l0); \
-    else if ((NTV) == 128) k_sweep_y<SPHV, TD, 128, 1><<<grid, 128, 0, s>>>(T, P, ph, c, l0);  \
-    else if ((NTV) == 64) k_sweep_y<SPHV, TD, 64, 1><<<grid, 64, 0, s>>>(T, P, ph, c, l0);     \
-    else k_sweep_y<SPHV, TD, 32, 1><<<grid, 32, 0, s>>>(T, P, ph, c, l0);                      \
-  } while (0)
+// Isentropic runs (EOS 1) use the MINB 1 kernels and no pencil packing.
+template <bool SPHV, bool TD, int EOS>
+static void launch_x(int nt, int occ8, dim3 grid, int l0, const Tables &T, const Planes &P, const Phys &ph,
+                     const SweepCtl &c, cudaStream_t s) {
+  if constexpr (EOS == 0) {
+    if (nt == 128 && occ8) { k_sweep_x<SPHV, TD, 128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, l0); return; }
+  }
+  if (nt == 128) k_sweep_x<SPHV, TD, 128, 1, EOS><<<grid, 128, 0, s>>>(T, P, ph, c, l0);
+  else if (nt == 64) k_sweep_x<SPHV, TD, 64, 1, EOS><<<grid, 64, 0, s>>>(T, P, ph, c, l0);
+  else k_sweep_x<SPHV, TD, 32, 1, EOS><<<grid, 32, 0, s>>>(T, P, ph, c, l0);
+}
+template <bool SPHV, bool TD, int EOS>
+static void launch_y(int nt, int occ8, dim3 grid, int l0, const Tables &T, const Planes &P, const Phys &ph,
+                     const SweepCtl &c, cudaStream_t s) {
+  if constexpr (EOS == 0) {
+    if (nt == 128 && occ8) { k_sweep_y<SPHV, TD, 128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, l0); return; }
+  }
+  if (nt == 128) k_sweep_y<SPHV, TD, 128, 1, EOS><<<grid, 128, 0, s>>>(T, P, ph, c, l0);
+  else if (nt == 64) k_sweep_y<SPHV, TD, 64, 1, EOS><<<grid, 64, 0, s>>>(T, P, ph, c, l0);
+  else k_sweep_y<SPHV, TD, 32, 1, EOS><<<grid, 32, 0, s>>>(T, P, ph, c, l0);
+}
+template <int EOS>
+static void launch_z(int nt, int occ8, dim3 grid, int l0, int ntop, const Tables &T, const Planes &P,
+                     const Phys &ph, const SweepCtl &c, cudaStream_t s) {
+  if constexpr (EOS == 0) {
+    if (nt == 128 && occ8) { k_sweep_z<128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, l0); return; }
+  }
+  if (nt == 128) k_sweep_z<128, 1, EOS><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, l0);
+  else if (nt == 64) k_sweep_z<64, 1, EOS><<<grid, 64, 0, s>>>(T, P, ph, c, ntop, l0);
+  else k_sweep_z<32, 1, EOS><<<grid, 32, 0, s>>>(T, P, ph, c, ntop, l0);
+}
 
-void sweep_x(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
+template <int EOS>
+static void sweep_x_t(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
   const Chunking &ch = T.cx;
   const int occ8 = T.occ8;
   int full = ch.stuck ? ch.loop : ch.loop - 1;
   if (full > 0) {
     dim3 grid(T.nphi, full, T.nk);
-    if (ndim == 3) PG_LAUNCH_X(true, true, 128, grid, 0);
-    else PG_LAUNCH_X(false, false, 128, grid, 0);
+    if (ndim == 3) launch_x<true, true, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
+    else launch_x<false, false, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
   }
   if (!ch.stuck) {
-    if (T.zpack && ch.lim_last <= PX_LIM) {
-      int npen = T.nphi * T.nk, blocks = (npen + 3) / 4, nt = 4 * ch.lim_last;
-      if (ndim == 3) k_sweep_x_packed<true, true, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
-      else k_sweep_x_packed<false, false, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
-      return;
+    if constexpr (EOS == 0) {
+      if (T.zpack && ch.lim_last <= PX_LIM) {
+        int npen = T.nphi * T.nk, blocks = (npen + 3) / 4, nt = 4 * ch.lim_last;
+        if (ndim == 3) k_sweep_x_packed<true, true, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
+        else k_sweep_x_packed<false, false, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
+        return;
+      }
     }
     dim3 grid(T.nphi, 1, T.nk);
     int nt = cta_for(ch.lim_last);
     int l0 = ch.loop - 1;
-    if (ndim == 3) PG_LAUNCH_X(true, true, nt, grid, l0);
-    else PG_LAUNCH_X(false, false, nt, grid, l0);
+    if (ndim == 3) launch_x<true, true, EOS>(nt, occ8, grid, l0, T, P, ph, c, s);
+    else launch_x<false, false, EOS>(nt, occ8, grid, l0, T, P, ph, c, s);
   }
 }
+void sweep_x(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
+  if (ph.eos) sweep_x_t<1>(T, P, ph, c, ndim, s);
+  else sweep_x_t<0>(T, P, ph, c, ndim, s);
+}
 
-void sweep_y(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
+template <int EOS>
+static void sweep_y_t(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
   const Chunking &ch = T.cy;
   const int occ8 = T.occ8;
   int full = ch.stuck ? ch.loop : ch.loop - 1;
   if (full > 0) {
     dim3 grid(full, T.nr, T.nk);
-    if (ndim == 3) PG_LAUNCH_Y(true, true, 128, grid, 0);
-    else PG_LAUNCH_Y(false, false, 128, grid, 0);
+    if (ndim == 3) launch_y<true, true, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
+    else launch_y<false, false, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
   }
   if (!ch.stuck) {
     dim3 grid(1, T.nr, T.nk);
     int nt = cta_for(ch.lim_last);
     int l0 = ch.loop - 1;
-    if (ndim == 3) PG_LAUNCH_Y(true, true, nt, grid, l0);
-    else PG_LAUNCH_Y(false, false, nt, grid, l0);
+    if (ndim == 3) launch_y<true, true, EOS>(nt, occ8, grid, l0, T, P, ph, c, s);
+    else launch_y<false, false, EOS>(nt, occ8, grid, l0, T, P, ph, c, s);
   }
 }
+void sweep_y(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
+  if (ph.eos) sweep_y_t<1>(T, P, ph, c, ndim, s);
+  else sweep_y_t<0>(T, P, ph, c, ndim, s);
+}
 
-void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s) {
+template <int EOS>
+static void sweep_z_t(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s) {
   const Chunking &ch = T.cz;
-  if (T.zpack && ch.loop == 1 && !ch.stuck && ch.lim_last <= PZ_LIM) {
-    int npen = T.nr * T.nphi;
-    k_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
-    return;
+  if constexpr (EOS == 0) {
+    if (T.zpack && ch.loop == 1 && !ch.stuck && ch.lim_last <= PZ_LIM) {
+      int npen = T.nr * T.nphi;
+      k_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
+      return;
+    }
   }
   int full = ch.stuck ? ch.loop : ch.loop - 1;
   if (full > 0) {
     dim3 grid(T.nr, T.nphi, full);
-    if (T.occ8) k_sweep_z<128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, 0);
-    else k_sweep_z<128, 1><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, 0);
+    launch_z<EOS>(128, T.occ8, grid, 0, ntop, T, P, ph, c, s);
   }
   if (!ch.stuck) {
     dim3 grid(T.nr, T.nphi, 1);
-    int nt = cta_for(ch.lim_last);
-    int l0 = ch.loop - 1;
-    if (nt == 32) k_sweep_z<32, 1><<<grid, 32, 0, s>>>(T, P, ph, c, ntop, l0);
-    else if (nt == 64) k_sweep_z<64, 1><<<grid, 64, 0, s>>>(T, P, ph, c, ntop, l0);
-    else if (T.occ8) k_sweep_z<128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, l0);
-    else k_sweep_z<128, 1><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, l0);
+    launch_z<EOS>(cta_for(ch.lim_last), T.occ8, grid, ch.loop - 1, ntop, T, P, ph, c, s);
   }
+}
+void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s) {
+  if (ph.eos) sweep_z_t<1>(T, P, ph, c, ntop, s);
+  else sweep_z_t<0>(T, P, ph, c, ntop, s);
 }
 
 // kernels launched by one sweep_* call
@@ -1460,10 +1490,10 @@ void fill_ghost_rows(const Tables &T, const double *ghosts, const DumpPlanes &D,
   dim3 grid((T.nphi + 255) / 256, 2 * NPAD, T.nk);
   k_fill_ghost_rows<<<grid, 256, 0, s>>>(T, ghosts, D, ndim, fp32);
 }
-void pack_dump(const Tables &T, const DumpPlanes &D, int ndim, int fp32, int p0_live, unsigned char *out,
+void pack_dump(const Tables &T, const DumpPlanes &D, const Phys &ph, int ndim, int fp32, int p0_live, unsigned char *out,
                cudaStream_t s) {
   dim3 grid((T.nphi + 255) / 256, T.nr, T.nk);
-  k_pack_dump<<<grid, 256, 0, s>>>(T, D, ndim, fp32, p0_live, out);
+  k_pack_dump<<<grid, 256, 0, s>>>(T, D, ph, ndim, fp32, p0_live, out);
 }
 
 void poststep(DevClock *clk, const Tables &T, cudaStream_t s) {

@@ -177,7 +177,7 @@ void unpack_dump(const Tables &T, const double *stage, const DumpPlanes &D, int 
                  cudaStream_t s);
 void fill_ghost_rows(const Tables &T, const double *ghosts, const DumpPlanes &D, int ndim, int fp32,
                      cudaStream_t s);
-void pack_dump(const Tables &T, const DumpPlanes &D, int ndim, int fp32, int p0_live, unsigned char *out,
+void pack_dump(const Tables &T, const DumpPlanes &D, const Phys &ph, int ndim, int fp32, int p0_live, unsigned char *out,
                cudaStream_t s);
 // post-processing (read/ tools): azimuthal harmonic m per ring of layer 0
 // (ab[2i], ab[2i+1]), torque on a planet at r = 1 per ring (ring_out[k*nr+i])

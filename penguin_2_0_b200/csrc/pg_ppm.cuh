@@ -13,8 +13,9 @@
 //    from a separate buffer, instead of one CTA walking the pencil with a
 //    6-cell carry (ppm.cu:43-157 carries pre-update values, so the result is
 //    the same Jacobi update);
-//  * the q = p/rho remap (remap.cu:123-131) is skipped: in EOS 0 the sweep
-//    store overwrites p with rho*cs2 (ppm.cu:139);
+//  * the q remap (remap.cu:123-142) and the q of evolve (evolve.cu:131-135)
+//    are skipped: the sweep store overwrites p by the EOS relation
+//    (ppm.cu:138-143), so they never reach the stored state;
 //  * in 2D the remap of the slot holding w is skipped (w stays exactly 0:
 //    the w slot of the radial sweep, the v slot of the azimuthal sweep) and
 //    umid *= pmid (evolve.cu:73, used by EOS 2 only) is dropped;
@@ -43,16 +44,60 @@ struct Body { double m, x, y, vx, vy, fx, fy, rs; };
 // Physics constants of the run (global.h), passed by value to kernels.
 struct Phys {
   double gam, sc2, vis_nu, p_alpha, p_beta;
+  double gamfac1, gamfac2;  // (gam + 1)/gam/2 and gam + 1 (global.h:54-55)
   int plnt;       // plnt_flag > 0
   int flat;       // flat_flag
   int visc;       // visc_flag
+  int eos;        // EOS: 0 isothermal, 1 isentropic (global.h:18)
 };
+
+// Pressure of a cell from its density by the sweep store's relation
+// (ppm.cu:138-143): EOS 0 p = rho cs2, EOS 1 p = cs2 rho^gam / gam.  The
+// planes hold no pressure; every reader of p derives it here.  The sweeps
+// take EOS as a template argument (the EOS-0 kernels carry no pow); the
+// small kernels around them (CFL, dump packing) branch at run time.
+template <int EOS>
+__device__ __forceinline__ double eos_p(double r, double cs2, const Phys &ph) {
+  if (EOS == 0) return r * cs2;
+  return cs2 * pow(r, ph.gam) / ph.gam;
+}
+__device__ __forceinline__ double eos_p_rt(double r, double cs2, const Phys &ph) {
+  return ph.eos ? eos_p<1>(r, cs2, ph) : eos_p<0>(r, cs2, ph);
+}
+
+// Isentropic Riemann problem (riemann.cu:75-111, the EOS 1 branch): van
+// Leer's (1979) Newton iteration for the contact pressure on the Lagrangian
+// sound speeds C = sqrt(gam p rho), at most 10 iterations, relative
+// tolerance 1e-8; the face velocity is the mean of the two wave fans'.
+__device__ __forceinline__ void riemann_isentropic(double pl, double rl, double ul, double pr, double rr,
+                                                   double ur, const Phys &ph, double &umid, double &pmid) {
+  const double cl = sqrt(ph.gam * pl * rl), cr = sqrt(ph.gam * pr * rr);
+  const double vl = 1.0 / rl, vr = 1.0 / rr;
+  double pm = pr - pl - cr * (ur - ul);
+  pm = pl + pm * cl / (cl + cr);
+  pm = fmax(kSmallp, pm);
+  double wl = 0.0, wr = 0.0;
+  for (int it = 0; it < 10; it++) {
+    const double prev = pm;
+    wl = cl * sqrt(1.0 + ph.gamfac1 * (pm - pl) / pl);
+    wr = cr * sqrt(1.0 + ph.gamfac1 * (pm - pr) / pr);
+    double zl = 4.0 * vl * wl * wl, zr = 4.0 * vr * wr * wr;
+    zl = -zl * wl / (zl - ph.gamfac2 * (pm - pl));
+    zr = zr * wr / (zr - ph.gamfac2 * (pm - pr));
+    const double uml = ul - (pm - pl) / wl, umr = ur + (pm - pr) / wr;
+    pm = pm + (umr - uml) * (zr * zl) / (zr - zl);
+    pm = fmax(kSmallp, pm);
+    if (fabs(pm - prev) / pm < 1.0e-8) break;
+  }
+  umid = 0.5 * ((ul - (pm - pl) / wl) + (ur + (pm - pr) / wr));
+  pmid = fmax(kSmallp, pm);
+}
 
 struct Par { double c0, c1, c2, c3, c4; };
 
 // Shared arrays of one chunk: the sweep kernel's (ppm.cu:38-39) and
 // ppmlr's (ppmlr.cu:7-10).  q only serves as parabola storage (al) because
-// the q = p/rho remap is dead in EOS 0.  NT is the CTA size: 128 for full
+// the q remap is dead in EOS 0 and 1.  NT is the CTA size: 128 for full
 // chunks, 64 or 32 for a short last chunk (lim <= NT).
 template <int NT>
 struct ChunkShmT {

@@ -234,6 +234,9 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
   run->ph.plnt = p->plnt_flag > 0;
   run->ph.flat = p->flat_flag != 0;
   run->ph.visc = p->visc_flag == 1;
+  run->ph.eos = p->EOS;
+  run->ph.gamfac2 = p->gam + 1.0;
+  run->ph.gamfac1 = run->ph.gamfac2 / p->gam / 2.0;
   *out = run;
   return PG_OK;
 }
@@ -466,7 +469,7 @@ int pg_save_rings(pg_run *run, void *rings, size_t bytes) {
     D.r = run->planes[c][0]; D.u = run->planes[c][1]; D.v = run->planes[c][2]; D.w = run->planes[c][3];
     D.p0 = run->p0;
   }
-  pgk::pack_dump(run->T, D, P.ndim, run->fp32, run->p0_live ? 1 : 0, stage, s);
+  pgk::pack_dump(run->T, D, run->ph, P.ndim, run->fp32, run->p0_live ? 1 : 0, stage, s);
   cudaError_t ce = cudaGetLastError();
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(rings, stage, bytes, cudaMemcpyDeviceToHost, s);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
@@ -1179,6 +1182,7 @@ int run_shape(const pg_run *run, RunShape *o) {
   o->clock_ready = run->clock_ready ? 1 : 0;
   o->p0_live = run->p0_live ? 1 : 0;
   o->moving = run->P.plnt_flag == 2 ? 1 : 0;
+  o->eos = run->P.EOS;
   o->nr = run->nr; o->nphi = run->nphi; o->nk = run->nk;
   const pgd::Chunking &cx = run->T.cx;
   const bool short_last = !cx.stuck && cx.lim_last <= 64;

@@ -12,7 +12,8 @@ Three stages:
          mass, torque) and Sigma, v_r, v_phi, rot_j of the saved steps, in
          the reference's storage order.
 
-usage: python tests/golden/make_golden.py build | run <rawdir> | pack <rawdir> [outdir [fulldir]]
+usage: python tests/golden/make_golden.py [--only=case,...] build | run <rawdir> | pack <rawdir> [outdir [fulldir]]
+(--only restricts build, run and pack to the named cases)
 """
 import ctypes as C
 import json
@@ -48,6 +49,9 @@ CASES = {
     # no planet, no viscosity, no flattening, no FARGO, no damping
     "g136x200_plain": (0, dict(imax=136, jmax=200, plnt_flag=0, visc_flag=0, flat_flag=0,
                                FARGO_flag=0, kill_rin=0.0, kill_rout=0.0), 6, (1, 6)),
+    # isentropic EOS 1, gam 1.4: the Newton Riemann solver (riemann.cu:75-111)
+    # and p = cs2 Sigma^gam / gam at every store; planet, viscosity, damping
+    "g136x200_eos1": (0, dict(imax=136, jmax=200, EOS=1, gam=1.4), 8, (1, 3, 8)),
 }
 
 
@@ -75,8 +79,15 @@ def to_json(p):
     return {k: (float(v).hex() if isinstance(v, float) else v) for k, v in p.as_dict().items()}
 
 
+ONLY = None   # --only=case,...: restrict the stages to these cases
+
+
+def _cases(names):
+    return [c for c in names if ONLY is None or c in ONLY]
+
+
 def cmd_build():
-    for case in list(CASES) + list(PERF_CASES):
+    for case in _cases(list(CASES) + list(PERF_CASES)):
         p = params_for(case)
         d = os.path.join(ROOT, "oracle", "_ref", case)
         os.makedirs(d, exist_ok=True)
@@ -113,7 +124,8 @@ def cmd_perf(rawdir):
 def cmd_run(rawdir):
     from penguin_2_0_b200 import _lib
     L = _lib.lib()
-    for case, (_, _, nsteps, keep) in CASES.items():
+    for case in _cases(CASES):
+        _, _, nsteps, keep = CASES[case]
         p = params_for(case)
         out = os.path.join(rawdir, case)
         os.makedirs(out, exist_ok=True)
@@ -146,7 +158,8 @@ def read_rings(path, p):
 
 
 def cmd_pack(rawdir, outdir=HERE, full=None):
-    for case, (_, _, nsteps, keep) in CASES.items():
+    for case in _cases(CASES):
+        _, _, nsteps, keep = CASES[case]
         p = params_for(case)
         src = os.path.join(rawdir, case)
         rows = [ln.split() for ln in open(os.path.join(src, "hist.txt"))]
@@ -174,6 +187,8 @@ def cmd_pack(rawdir, outdir=HERE, full=None):
 
 
 if __name__ == "__main__":
+    if sys.argv[1].startswith("--only="):
+        ONLY = set(sys.argv.pop(1).split("=", 1)[1].split(","))
     what = sys.argv[1]
     if what == "build":
         cmd_build()

@@ -37,7 +37,11 @@ def test_default_params_are_global_h():
 
 @pytest.mark.parametrize("over,ok", [
     (dict(), True),
-    (dict(EOS=1), False),
+    (dict(EOS=1, gam=1.4), True),        # isentropic (riemann.cu:75-111)
+    (dict(EOS=1, gam=1.0), True),        # 2D isentropic at gam 1
+    (dict(EOS=2, gam=1.4), False),       # energy equation: marked buggy by the reference
+    (dict(EOS=1, gam=1.4, precision=1), False),  # FP32 planes: EOS 0 only
+    (dict(EOS=0, gam=0.9), False),
     (dict(bary_flag=1), False),
     (dict(jmax=116 * 3 + 3), False),     # azimuthal wrap would read updated cells
     (dict(jmax=116 * 3), True),          # last chunk idle, reproduced
@@ -77,18 +81,61 @@ def test_ic_is_seeded_and_consistent():
 def test_label_matches_create_label():
     p = pg.params(0)
     assert pg.label(p) == "256x768x1_c50_p333_s60_i40_o250_a10_b10_rot_fargo"
+    # EOS 1 names gamma instead of the temperature slope (output.cu:72-79)
+    assert pg.label(pg.params(0, EOS=1, gam=1.4)) == "256x768x1_c50_p333_s60_i40_o250_a10_g14_rot_fargo"
 
 
-def test_dump_name_and_time_file(tmp_path):
-    import ctypes as C
-    p = pg.params(0)
-    L = _lib.lib()
-    b = C.create_string_buffer(512)
-    assert L.pg_dump_name(C.byref(p), b"binary", 7, b, 512) == 0
-    assert b.value.decode() == "binary/binary_256x768x1_c50_p333_s60_i40_o250_a10_b10_rot_fargo_00007"
-    rows = np.arange(22, dtype=np.float64).reshape(2, 11) + 0.5
-    path = str(tmp_path / "time.dat")
-    assert L.pg_write_time_rows(path.encode(), rows.ctypes.data_as(C.POINTER(C.c_double)), 2, 0) == 0
-    back = np.loadtxt(path)
-    np.testing.assert_array_equal(back, rows)
-    assert open(path).readline().startswith("0.5 1.5 2.5")
+def test_3d_isentropic_needs_gam_above_one():
+    assert pg.host.check_params(pg.params(1, EOS=1, gam=1.0)) != 0
+    assert pg.host.check_params(pg.params(1, EOS=1, gam=5.0 / 3.0)) == 0
+
+
+def test_isentropic_ic_pressure_and_profile():
+    # p = cs2 Sigma^gam / gam (the EOS-1 store, ppm.cu:140-141); the 2D
+    # surface density keeps its r^-p_alpha slope (disk_profile.cu:9-28) and
+    # v_phi^2 = 1/r + r dP/dr / Sigma with the isentropic P(r)
+    gam = 1.4
+    p = pg.params(0, imax=130, jmax=240, EOS=1, gam=gam)
+    f = pg.dump_fields(pg.build_ic(p), p)
+    cs2 = 0.05 ** 2 / f["xc"][:, None]
+    np.testing.assert_allclose(f["p"], cs2 * f["r"] ** gam / gam, rtol=1e-15)
+    dev = f["r"] / f["xc"][:, None] ** -1.0 - 1.0
+    assert np.all(np.abs(dev) <= 1e-4 * (1 + 1e-12))
+    r = f["xc"]
+    P = lambda x: 0.05 ** 2 / x * (x ** -1.0) ** gam / gam
+    dP = (P(r + 1.27245e-8) - P(r - 1.27245e-8)) / 2.5449e-8
+    vk = np.sqrt(1.0 / r + r * dP / r ** -1.0)
+    # the centred difference over 2.5e-8 turns last-ulp pow differences
+    # (numpy vs libm) into ~1e-11 of v_phi
+    np.testing.assert_allclose(f["v"][:, 0], vk, rtol=1e-10)
+    # differs from the isothermal disk's rotation
+    f0 = pg.dump_fields(pg.build_ic(pg.params(0, imax=130, jmax=240)), p)
+    assert np.max(np.abs(f0["v"][:, 0] / f["v"][:, 0] - 1.0)) > 1e-5
+
+
+def test_isentropic_3d_ic_is_the_polytrope():
+    # rho(r, z)^(gam-1) = rho_mid^(gam-1) - (gam-1)/(r cs2) (1 - r/sqrt(r^2+z^2))
+    # below z_0, continued above z_0 by a decade per h/6 (disk_profile.cu:86-103),
+    # with rho_mid ~ r^(-p_alpha 2/(gam+1))
+    gam = 5.0 / 3.0
+    p = pg.params(1, imax=64, jmax=132, kmax=16, EOS=1, gam=gam)
+    f = pg.dump_fields(pg.build_ic(p), p)
+    nr, nk = p.imax, p.kmax
+    sig = f["r"].reshape(nk, nr, -1)
+    xc = f["xc"].reshape(nk, nr)[0]
+    zc = f["zc"].reshape(nk, nr)[:, 0]
+    gm = gam - 1.0
+    below = above = 0
+    for k in range(nk):
+        R = xc * np.sin(zc[k])
+        Z = xc * np.cos(zc[k])
+        c2 = 0.05 ** 2 * R ** -1.0
+        h = np.sqrt(c2 * R ** 3)
+        z0 = np.sqrt(2 * h * h * R ** (-1.5 * (2 / (gam + 1)) * gm) / gm)
+        mid = R ** (-1.5 * 2 / (gam + 1))
+        poly = lambda zz: (mid ** gm - gm / (R * c2) * (1 - R / np.sqrt(R * R + zz * zz))) ** (1 / gm)
+        want = np.where(Z < z0, poly(np.minimum(Z, z0)), 10.0 ** (np.log10(poly(z0)) - 6.0 * (Z - z0) / h))
+        below += int(np.sum(Z < z0))
+        above += int(np.sum(Z >= z0))
+        np.testing.assert_allclose(sig[k, :, 0], want, rtol=1.1e-4)   # the seeded noise is 1e-4
+    assert below > 0 and above > 0

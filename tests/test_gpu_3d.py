@@ -19,7 +19,8 @@ def _p(**over):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("over", [dict(), dict(ntop=3), dict(plnt_flag=0, visc_flag=0)])
+@pytest.mark.parametrize("over", [dict(), dict(ntop=3), dict(plnt_flag=0, visc_flag=0),
+                                  dict(EOS=1, gam=5.0 / 3.0)])
 def test_3d_host_loop_matches_oracle(gpu, over):
     p = _p(**over)
     ic = pg.build_ic(p)
@@ -45,8 +46,9 @@ def test_3d_host_loop_matches_oracle(gpu, over):
 
 
 @pytest.mark.gpu
-def test_3d_fused_loop_equals_host_loop(gpu):
-    p = _p()
+@pytest.mark.parametrize("over", [dict(), dict(EOS=1, gam=5.0 / 3.0)])
+def test_3d_fused_loop_equals_host_loop(gpu, over):
+    p = _p(**over)
     ic = pg.build_ic(p)
     with pg.Run(p, 0) as a, pg.Run(p, 0) as b:
         a.load(ic)

@@ -20,6 +20,7 @@ CASES = [
     dict(which=0, imax=136, jmax=408, plnt_flag=0, precision=1),
     dict(which=1, imax=64, jmax=132, kmax=16),
     dict(which=0, imax=136, jmax=408, plnt_flag=2),             # moving planet: own launch sequence
+    dict(which=0, imax=136, jmax=408, EOS=1, gam=1.4),          # isentropic: own launch sequence
 ]
 
 

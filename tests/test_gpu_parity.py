@@ -22,6 +22,9 @@ CASES = {
                            kill_rin=0.0, kill_rout=0.0),
     "cfg0": dict(imax=256, jmax=768),
     "g136x136_moving": dict(imax=136, jmax=136, plnt_flag=2),   # the planet feels the disk (global.h default)
+    # isentropic EOS 1 (Newton Riemann solver, p = cs2 Sigma^gam / gam)
+    "g136x136_eos1": dict(imax=136, jmax=136, EOS=1, gam=1.4),
+    "cfg0_eos1": dict(imax=256, jmax=768, EOS=1, gam=5.0 / 3.0),
 }
 
 
@@ -67,8 +70,9 @@ def test_host_loop_matches_oracle(gpu, case):
 
 
 @pytest.mark.gpu
-def test_fused_loop_equals_host_loop(gpu):
-    p = _params(dict(imax=256, jmax=768))
+@pytest.mark.parametrize("eos", [dict(), dict(EOS=1, gam=1.4)])
+def test_fused_loop_equals_host_loop(gpu, eos):
+    p = _params(dict(imax=256, jmax=768, **eos))
     ic = pg.build_ic(p)
     with pg.Run(p, 0) as a, pg.Run(p, 0) as b:
         a.load(ic)
@@ -99,6 +103,23 @@ def test_graph_equals_stream_loop(gpu):
         ha, hb = a.history(), b.history()
         np.testing.assert_array_equal(ha, hb)
         assert ha.shape[0] == 9
+
+
+@pytest.mark.gpu
+def test_isentropic_dump_pressure(gpu):
+    # the saved p of an EOS-1 run is the store's cs2 Sigma^gam / gam
+    # (ppm.cu:140-141), derived on the device from the planes
+    gam = 1.4
+    p = _params(dict(imax=136, jmax=136, EOS=1, gam=gam))
+    with pg.Run(p, 0) as run:
+        run.load(pg.build_ic(p))
+        run.clock_reset(0)
+        run.advance(3)
+        f = pg.dump_fields(run.save(), p)
+    cs2 = p.sc_h ** 2 * f["xc"][:, None] ** -p.p_beta
+    # CUDA's pow is within 2 ulp, libm's within 1; the product and the
+    # division add a rounding each: 6 ulp
+    np.testing.assert_allclose(f["p"], cs2 * f["r"] ** gam / gam, rtol=6 * 2.0 ** -53 * 2)
 
 
 @pytest.mark.gpu

@@ -25,12 +25,15 @@ as one region.
 roofline: the dominant kernel's algorithmic bytes (3 fields read + 3 written
 in FP64 = 48 B per cell per 2D sweep, 4 fields = 64 B in 3D) over its mean
 event-timed duration, against MEASURED_PEAKS.json's HBM copy bandwidth.
-e2e: the same metric through the reference-facing calls of the C ABI: the
-seeded dump is loaded from pinned host memory (pg_load_rings), the steps run
-through pg_get_dt, pg_index_shift, pg_sweep2d/3d, pg_damp and pg_reduce with
-main.cu's host syncs (dt, planet and FrRot to the device, dt, mass and torque
-back every step), and the final dump is saved to pinned host memory, all
-inside the timed region.
+e2e: the same metric for a job through the C ABI with host buffers: the
+seeded dump is loaded from pinned host memory (pg_load_rings), pg_clock_reset
+and pg_advance_graph (the ABI's replacement of main.cu's loop) run the steps,
+every step's diagnostics row (dt, mass, torque, ...) is read back (pg_history)
+and the final dump is saved to pinned host memory, all inside the timed
+region.  e2e_host_loop times the reference's per-call sequence instead
+(pg_get_dt, pg_index_shift, pg_sweep2d/3d, pg_damp, pg_reduce from a Python
+loop with main.cu's host syncs: dt, planet and FrRot to the device, dt, mass
+and torque back every step).
 cpu_baseline: the CPU oracle (a restatement of the reference's sweeps in C,
 OpenMP over the box's cores) on a bounded sample of the same workload.
 """
@@ -464,34 +467,58 @@ def main():
             if line.startswith("traffic_bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
 
-    # e2e through the reference-facing calls: the dump goes in from pinned host
-    # memory (pg_load_rings), the host-driven loop runs with the reference's
-    # syncs (dt, planet and FrRot to the device, dt, mass and torque back every
-    # step), and the final dump comes back (pg_save_rings), all timed
+    # e2e: a job through the C ABI with host buffers.  The dump goes in from
+    # pinned host memory (pg_load_rings), pg_clock_reset + pg_advance_graph run
+    # the steps (the ABI's replacement of main.cu:343-441), the diagnostics row
+    # of every step (simtime, dt, mass, torque, ...; nprin 1) comes back with
+    # pg_history and the final dump with pg_save_rings (pinned), all timed.
+    # The host-driven loop of the reference's per-call sequence (pg_get_dt,
+    # pg_index_shift, pg_sweep*, pg_damp, pg_reduce with main.cu's host syncs)
+    # is timed the same way as e2e_host_loop.
     import numpy as np
     e2e_steps = max(3, min(args.steps // 10, 200))
     dump_bytes = len(ic)
     pin_in = torch.empty(dump_bytes, dtype=torch.uint8, pin_memory=True)
     pin_in.numpy()[:] = np.frombuffer(bytes(ic), dtype=np.uint8)
     pin_out = torch.empty(dump_bytes, dtype=torch.uint8, pin_memory=True)
-    run2 = pg.Run(p, local).load(ic)
-    run2.kernel_loop(2)
+    pe = pg.params(None)
+    pe.update(**p.as_dict())
+    pe.nprin = 1
+    run2 = pg.Run(pe, local).load(ic)
+    run2.clock_reset(0)
+    run2.advance(args.chunk, graph_chunk=args.chunk)     # graph capture outside the timed job
     torch.cuda.synchronize()
-
-    def rec(s, simtime, dt_used, planet, FrRot):
-        pg.GPU_output_reduction(run2, planet, 0.0, 0)
-        if p.plnt_flag:
-            pg.GPU_output_reduction(run2, planet, 0.0, 9)
-
     _barrier(dist)
     t0 = time.perf_counter()
     run2.load_from(pin_in.data_ptr(), dump_bytes)
-    run2.kernel_loop(e2e_steps, record=rec)
+    run2.clock_reset(0)
+    done = run2.advance(e2e_steps, graph_chunk=args.chunk)
+    hist = run2.history(max_rows=e2e_steps)
     run2.save_to(pin_out.data_ptr(), dump_bytes)
     torch.cuda.synchronize()
     e2e_el = _max_over_ranks(dist, time.perf_counter() - t0)
+    assert done == e2e_steps and hist.shape[0] == e2e_steps, (done, hist.shape)
     e2e_value = cells * e2e_steps * ws / e2e_el
     run2.close()
+
+    run3 = pg.Run(p, local).load(ic)
+    run3.kernel_loop(2)
+    torch.cuda.synchronize()
+
+    def rec(s, simtime, dt_used, planet, FrRot):
+        pg.GPU_output_reduction(run3, planet, 0.0, 0)
+        if p.plnt_flag:
+            pg.GPU_output_reduction(run3, planet, 0.0, 9)
+
+    _barrier(dist)
+    t0 = time.perf_counter()
+    run3.load_from(pin_in.data_ptr(), dump_bytes)
+    run3.kernel_loop(e2e_steps, record=rec)
+    run3.save_to(pin_out.data_ptr(), dump_bytes)
+    torch.cuda.synchronize()
+    hl_el = _max_over_ranks(dist, time.perf_counter() - t0)
+    hl_value = cells * e2e_steps * ws / hl_el
+    run3.close()
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -516,11 +543,18 @@ def main():
                          "mean_launch_ms": mean[top], "kernels_ms": mean},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "zone-updates/s",
-                    "h2d_bytes_per_step": (dump_bytes + (64 + 16) * e2e_steps) / e2e_steps,
-                    "d2h_bytes_per_step": (dump_bytes + (8 + 8 + 8) * e2e_steps) / e2e_steps,
+                    "h2d_bytes_per_step": dump_bytes / e2e_steps,
+                    "d2h_bytes_per_step": (dump_bytes + 8 * 11 * e2e_steps) / e2e_steps,
                     "steps": e2e_steps,
-                    "path": "pg_load_rings from pinned host memory, host loop over pg_get_dt/pg_index_shift/"
-                            "pg_sweep2d|3d/pg_damp/pg_reduce, pg_save_rings to pinned host memory"},
+                    "path": "pg_load_rings from pinned host memory, pg_clock_reset + pg_advance_graph "
+                            "(device-resident loop, nprin 1), pg_history rows, pg_save_rings to pinned host memory"},
+            "e2e_host_loop": {"value": hl_value, "unit": "zone-updates/s",
+                              "h2d_bytes_per_step": (dump_bytes + (64 + 16) * e2e_steps) / e2e_steps,
+                              "d2h_bytes_per_step": (dump_bytes + (8 + 8 + 8) * e2e_steps) / e2e_steps,
+                              "steps": e2e_steps,
+                              "path": "pg_load_rings from pinned host memory, host loop (Python) over pg_get_dt/"
+                                      "pg_index_shift/pg_sweep2d|3d/pg_damp/pg_reduce with main.cu's syncs, "
+                                      "pg_save_rings to pinned host memory"},
             "gpu_launches": int(launches),
             "clocks": clk,
         }

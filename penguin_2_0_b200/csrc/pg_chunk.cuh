@@ -17,7 +17,8 @@ struct CellIn {
   double pol;    // polar angle (0 in 2D)
   double vrot;   // res_v / rad_cyl of the cell's ring
   double dvol0;  // Eulerian cell volume along the sweep
-  double sinpol; // sin(pol), formed once per cell (radial and azimuthal sweeps in 3D)
+  double sinpol; // sin(pol) of the cell (3D; the polar sweep's from a per-layer table)
+  double cospol; // cos(pol) of the cell (polar sweep)
 };
 
 // x^2 where the reference writes pow(x, 2)
@@ -65,21 +66,29 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
   }
 }
 
-// get_fx / get_fy / get_fz at a cell centre (forces.cu:226-372)
-template <int AXIS, bool SPH, class SHM>
+// get_fx / get_fy / get_fz at a cell centre (forces.cu:226-372).  CF0: the
+// planet's cos(azi - p.y) comes in as cf0 (the dt = 0 force of a radial or
+// polar pencil, one value per pencil).  The polar form takes sin and cos of
+// its angle from the caller (sp, cp).
+template <int AXIS, bool SPH, bool CF0 = false, class SHM>
 __device__ __forceinline__ double centre_force(int n, double dt, double rad, double azi, double pol,
-                                               double sinpol, const SHM &S, const Body &pl, const Phys &ph) {
+                                               double sinpol, const SHM &S, const Body &pl, const Phys &ph,
+                                               double cf0 = 0.0, double sp = 0.0, double cp = 0.0) {
   if (AXIS == 0) {
     double grav;
     const double ir = 1.0 / rad, ir2 = __dmul_rn(ir, ir), ir3 = __dmul_rn(ir2, ir);
     if (!SPH) {
-      if (ph.plnt) { grav = grav_rad_cyl(rad, azi, pol, pl, dt); grav += -ir2; }
+      if (ph.plnt) {
+        grav = CF0 ? grav_rad_cyl_cf(rad, cf0, pol, pl) : grav_rad_cyl(rad, azi, pol, pl, dt);
+        grav += -ir2;
+      }
       else { double dis = sqrt(rad * rad + pol * pol); grav = -rad / dis / dis / dis; }
       double f = grav;
       f += __dmul_rn(__dmul_rn(S.v[n], S.v[n]), ir3);
       return f;
     } else {
-      grav = ph.plnt ? grav_rad_sph_s(rad, azi, sinpol, pl, dt) : -ir2;
+      if (ph.plnt) grav = CF0 ? grav_rad_sph_cf(rad, cf0, sinpol, pl) : grav_rad_sph_s(rad, azi, sinpol, pl, dt);
+      else grav = -ir2;
       double f = grav;
       f += __dmul_rn(__dmul_rn(S.w[n], S.w[n]), ir3);
       f += __dmul_rn(__dmul_rn(S.v[n], S.v[n]), ir) / sq(rad * sinpol);
@@ -89,8 +98,9 @@ __device__ __forceinline__ double centre_force(int n, double dt, double rad, dou
     if (!SPH) return ph.plnt ? grav_azi_cyl(rad, azi, pol, pl, dt) : 0.0;
     return ph.plnt ? grav_azi_sph_s(rad, azi, sinpol, pl, dt) : 0.0;
   } else {
-    const double sp = sin(pol), cp = cos(pol);
-    double grav = ph.plnt ? grav_pol_sph_s(rad, azi, sp, cp, pl, dt) : 0.0;
+    (void)pol;
+    double grav = 0.0;
+    if (ph.plnt) grav = CF0 ? grav_pol_sph_cf(rad, cf0, sp, cp, pl) : grav_pol_sph_s(rad, azi, sp, cp, pl, dt);
     double irc = 1.0 / (rad * sp);
     double f = grav;
     f += __dmul_rn(S.w[n] * S.w[n] * cp, __dmul_rn(__dmul_rn(irc, irc), irc));
@@ -216,20 +226,27 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
     xa = vfac[n];
   }
   __syncthreads();
+  // polar sweep: sin of the new centre angle, reused by the volume below
+  double sxcl = 0.0;
   if (n >= 3 && n < nmax - 3) {
     double xcl = xa + 0.5 * S.dx[n];
     if (AXIS == 0) {
-      fto1 = centre_force<0, SPH>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S, pl, ph);
+      fto1 = centre_force<0, SPH, true>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S, pl, ph, S.cf0);
       fto2 = centre_force<0, SPH>(n, dt, xcl, c.azi + dt * c.vrot, c.pol, c.sinpol, S, pl, ph);
     } else if (AXIS == 1) {
       fto1 = centre_force<1, SPH>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S, pl, ph);
       fto2 = centre_force<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, c.sinpol, S, pl, ph);
     } else {
-      fto1 = centre_force<2, SPH>(n, 0.0, c.rad, c.azi, c.pol, 0.0, S, pl, ph);
-      fto2 = centre_force<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, 0.0, S, pl, ph);
+      fto1 = centre_force<2, SPH, true>(n, 0.0, c.rad, c.azi, c.pol, 0.0, S, pl, ph, S.cf0, c.sinpol, c.cospol);
+      sxcl = sin(xcl);
+      fto2 = centre_force<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, 0.0, S, pl, ph, 0.0, sxcl, cos(xcl));
     }
   }
   __syncthreads();
+  // polar sweep: the two sines of the volume factor, reused by the remap's
+  // overlap volume (same angles)
+  double sA = 0.0, sB = 0.0;
+  bool haveS = false;
   if (n >= 3 && n < nmax - 2) {
     double dxn = S.dx[n];
     if (AXIS == 0) {
@@ -245,9 +262,15 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
       // 2 sin((a+b)/2) sin((b-a)/2): the same value without the
       // cancellation that makes the reference's form depend on libm ulps
       double delx = xa - xa0n;
-      dvol = 2.0 * sin(xa + 0.5 * dxn) * sin(0.5 * dxn) * c.rad;
+      const double sc = (n < nmax - 3) ? sxcl : sin(xa + 0.5 * dxn);
+      dvol = 2.0 * sc * sin(0.5 * dxn) * c.rad;
       if (delx == 0.0) vfac[n] = sin(xa);
-      else vfac[n] = 2.0 * sin(xa0n + 0.5 * delx) * sin(0.5 * delx) / delx;
+      else {
+        sA = sin(xa0n + 0.5 * delx);
+        sB = sin(0.5 * delx);
+        haveS = true;
+        vfac[n] = 2.0 * sA * sB / delx;
+      }
     }
   }
   __syncthreads();
@@ -272,7 +295,8 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   } else {
     // remap.cu:53, cancellation-free form of (cos(xa0) - cos(xa)) * rad
     double d = xa - xa0n;
-    lvol = 2.0 * sin(xa0n + 0.5 * d) * sin(0.5 * d) * c.rad;
+    if (haveS) lvol = 2.0 * sA * sB * c.rad;
+    else lvol = 2.0 * sin(xa0n + 0.5 * d) * sin(0.5 * d) * c.rad;
   }
   double dxf = xa - xa0n;
   const bool delC = (dxf >= 0.0);

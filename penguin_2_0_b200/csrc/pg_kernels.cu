@@ -102,8 +102,11 @@ __device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, int n, bool store
     rad_cyl = T.radc[rk];
     c.azi = T.yc[j0];
     c.pol = THREED ? T.zc[k + NPAD] : 0.0;
-    c.sinpol = THREED ? sin(c.pol) : 0.0;
+    c.sinpol = THREED ? T.szc[k + NPAD] : 0.0;
+    c.cospol = 0.0;
     c.dvol0 = T.rxvol[row];
+    // the pencil's planet angle factor at the start of the step, once
+    if (n == 0) S.cf0 = ph.plnt ? planet_cosfac(c.azi, st.pl, 0.0) : 0.0;
     c.vrot = T.res_v[rk] / rad_cyl;
     S.xa0[n] = T.rx[row];
     S.dx0[n] = T.rdx[row];
@@ -116,7 +119,7 @@ __device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, int n, bool store
     bool ghost = (row < NPAD) || (row >= T.nr + NPAD);
     S.p[n] = ghost ? T.gp[rk] : (P.p0 ? P.p0[idx] : eos_p<EOS>(r, T.cs2[rk], ph));
   } else {
-    c.rad = 1.0; c.azi = 0.0; c.pol = 0.0; c.dvol0 = 1.0; c.vrot = 0.0; c.sinpol = 0.0;
+    c.rad = 1.0; c.azi = 0.0; c.pol = 0.0; c.dvol0 = 1.0; c.vrot = 0.0; c.sinpol = 0.0; c.cospol = 0.0;
   }
   __syncthreads();
   ppm_chunk<0, SPH, THREED, EOS>(S, n, lim, st.dt, st.frrot, c, st.pl, ph);
@@ -261,7 +264,8 @@ __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, cons
     CellIn c;
     c.rad = rad_cyl;
     c.pol = THREED ? T.zc[k + NPAD] : 0.0;
-    c.sinpol = THREED ? sin(c.pol) : 0.0;
+    c.sinpol = THREED ? T.szc[k + NPAD] : 0.0;
+    c.cospol = 0.0;
     c.vrot = T.res_v[rk] / rad_cyl;
     c.azi = 0.0; c.dvol0 = 1.0;
     if (act) {
@@ -390,7 +394,9 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
   CellIn c;
   c.rad = rad;
   c.azi = T.yc[j0];
-  c.pol = 0.0; c.vrot = 0.0; c.dvol0 = 1.0; c.sinpol = 0.0;
+  c.pol = 0.0; c.vrot = 0.0; c.dvol0 = 1.0; c.sinpol = 0.0; c.cospol = 0.0;
+  // the pencil's planet angle factor at the start of the step, once
+  if (n == 0) S.cf0 = ph.plnt ? planet_cosfac(c.azi, st.pl, 0.0) : 0.0;
   double rad_cyl = 1.0;
   size_t idx = 0;
   if (act) {
@@ -429,6 +435,8 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
       c.vrot = T.res_v[rkk] / rad_cyl;
     }
     c.pol = zc;
+    c.sinpol = T.szc[kr + NPAD];      // sin, cos of the layer's centre angle
+    c.cospol = T.czc[kr + NPAD];
     c.dvol0 = zvol * rad;
     S.xa0[n] = za;
     S.dx0[n] = dz;
@@ -548,6 +556,11 @@ __global__ void k_tables(Tables T, Phys ph, int ndim, double kill_rin, double ki
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int n = T.nk * T.nrg;
   if (t >= n) return;
+  if (t < T.nk + 2 * NPAD) {
+    // sin, cos of every polar layer's centre angle (ghost layers included)
+    const_cast<double *>(T.szc)[t] = sin(T.zc[t]);
+    const_cast<double *>(T.czc)[t] = cos(T.zc[t]);
+  }
   int k = t / T.nrg, row = t % T.nrg;
   double rad = T.rxc[row];
   double rc = rad;

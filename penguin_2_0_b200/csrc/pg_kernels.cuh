@@ -35,6 +35,7 @@ struct Tables {
   const double *gp;                             // [nk*nrg] ghost-ring pressure
   const double *y, *dy, *yvol, *yc;             // [nphi]
   const double *z, *dz, *zvol, *zc;             // [nk + 12]: 6 ghost layers each side
+  const double *szc, *czc;                      // [nk + 12]: sin(zc), cos(zc) (k_tables)
   const double *val_r, *val_u, *val_v;          // [nk*nrg] damping / FARGO targets
   const double *damp_g, *damp_pw;               // [nk*nrg] zone factor, r^-1.5
   const double *tg;                             // [6*nr*4] theta ghost state (udr): r,p,u,v

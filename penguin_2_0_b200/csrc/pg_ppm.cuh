@@ -103,15 +103,26 @@ template <int NT>
 struct ChunkShmT {
   double r[NT + 2], p[NT + 2], u[NT + 2], v[NT + 2], w[NT + 2], xa0[NT + 2], dx0[NT + 2];
   double q[NT + 2], dx[NT + 2], umid[NT + 2], pmid[NT + 2], tmp1[NT + 2];
+  // cos(phi - phi_planet) at the start of the step: one value for a radial
+  // or polar pencil, whose cells share the azimuth phi (written by cell 0)
+  double cf0;
 };
 
 // ---- star + planet gravity, forces.cu:23-182 (non-barycentric frame) ------
-__device__ __forceinline__ double grav_rad_cyl(double rad, double azi, double z, const Body &p, double dt) {
-  double cosfac = cos(azi - (p.y + dt * p.vy));
+// The *_cf forms take cosfac = cos(azi - (p.y + dt p.vy)) from the caller
+// (shared by the cells of a pencil at dt = 0); the arithmetic after it is
+// the same as in the forms that evaluate it.
+__device__ __forceinline__ double planet_cosfac(double azi, const Body &p, double dt) {
+  return cos(azi - (p.y + dt * p.vy));
+}
+__device__ __forceinline__ double grav_rad_cyl_cf(double rad, double cosfac, double z, const Body &p) {
   double plm = p.m;
   double plx = p.x;
   double Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + z * z + p.rs * p.rs);
   return -plm * (rad - plx * cosfac) / (Rp * Rp * Rp) - plm * cosfac / (plx * plx);
+}
+__device__ __forceinline__ double grav_rad_cyl(double rad, double azi, double z, const Body &p, double dt) {
+  return grav_rad_cyl_cf(rad, planet_cosfac(azi, p, dt), z, p);
 }
 __device__ __forceinline__ double grav_azi_cyl(double rad, double azi, double z, const Body &p, double dt) {
   double cosfac = cos(azi - (p.y + dt * p.vy));
@@ -145,14 +156,16 @@ __device__ __forceinline__ double grav_azi_sph(double rad, double azi, double po
 }
 // the same two forces with sin(pol) formed by the caller (once per cell when
 // pol is the cell's fixed polar angle): identical arithmetic otherwise
-__device__ __forceinline__ double grav_rad_sph_s(double rad, double azi, double sinpol, const Body &p, double dt) {
-  double cosfac = cos(azi - (p.y + dt * p.vy));
+__device__ __forceinline__ double grav_rad_sph_cf(double rad, double cosfac, double sinpol, const Body &p) {
   double stm = 1.0 / (1.0 + p.m);
   double plm = p.m * stm;
   double plx = p.x;
   double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac * sinpol;
   Rp = sqrt(Rp + p.rs * p.rs);
   return -plm * (rad - plx * cosfac * sinpol) / (Rp * Rp * Rp) - stm / (rad * rad) - plm * sinpol * cosfac / (plx * plx);
+}
+__device__ __forceinline__ double grav_rad_sph_s(double rad, double azi, double sinpol, const Body &p, double dt) {
+  return grav_rad_sph_cf(rad, planet_cosfac(azi, p, dt), sinpol, p);
 }
 __device__ __forceinline__ double grav_azi_sph_s(double rad, double azi, double sinpol, const Body &p, double dt) {
   double cosfac = cos(azi - (p.y + dt * p.vy));
@@ -165,9 +178,8 @@ __device__ __forceinline__ double grav_azi_sph_s(double rad, double azi, double 
   Rp = sqrt(Rp + p.rs * p.rs);
   return -plm * plx * sinfac / (Rp * Rp * Rp) + plm * sinpol * sinfac / plx / plx;
 }
-__device__ __forceinline__ double grav_pol_sph_s(double rad, double azi, double sinpol, double cospol,
-                                                 const Body &p, double dt) {
-  double cosfac = cos(azi - (p.y + dt * p.vy));
+__device__ __forceinline__ double grav_pol_sph_cf(double rad, double cosfac, double sinpol, double cospol,
+                                                  const Body &p) {
   double stm = 1.0 / (1.0 + p.m);
   double plm = p.m * stm;
   double plx = p.x;
@@ -175,6 +187,10 @@ __device__ __forceinline__ double grav_pol_sph_s(double rad, double azi, double 
   double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac * sinpol;
   Rp = sqrt(Rp + p.rs * p.rs);
   return plm * plx * cosfac * cospol / (Rp * Rp * Rp) - plm * cosfac * cospol / (sinpol * plx * plx);
+}
+__device__ __forceinline__ double grav_pol_sph_s(double rad, double azi, double sinpol, double cospol,
+                                                 const Body &p, double dt) {
+  return grav_pol_sph_cf(rad, planet_cosfac(azi, p, dt), sinpol, cospol, p);
 }
 __device__ __forceinline__ double grav_pol_sph(double rad, double azi, double pol, const Body &p, double dt) {
   double cosfac = cos(azi - (p.y + dt * p.vy));

@@ -19,6 +19,8 @@ struct CellIn {
   double dvol0;  // Eulerian cell volume along the sweep
   double sinpol; // sin(pol) of the cell (3D; the polar sweep's from a per-layer table)
   double cospol; // cos(pol) of the cell (polar sweep)
+  double sinfz;  // sin, cos of the cell's left face angle (polar sweep, per-layer table)
+  double cosfz;
 };
 
 // x^2 where the reference writes pow(x, 2)
@@ -54,10 +56,10 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
     if (!SPH) ftot = ph.plnt ? grav_azi_cyl(c.rad, azi, c.pol, pl, hdt) : 0.0;
     else ftot = ph.plnt ? grav_azi_sph_s(c.rad, azi, c.sinpol, pl, hdt) : 0.0;
   } else {
-    // get_fz_bound forces.cu:298-334 (ngeomz 5) at the face angle xa0[n]
-    double pol = S.xa0[n];
+    // get_fz_bound forces.cu:298-334 (ngeomz 5) at the face angle xa0[n],
+    // whose sin and cos come from the per-layer table
     double azi = c.azi + hdt * c.vrot;
-    const double sp = sin(pol), cp = cos(pol);
+    const double sp = c.sinfz, cp = c.cosfz;
     double grav = ph.plnt ? grav_pol_sph_s(c.rad, azi, sp, cp, pl, hdt) : 0.0;
     double irc = 1.0 / (c.rad * sp);
     double f = grav;

@@ -394,7 +394,7 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
   CellIn c;
   c.rad = rad;
   c.azi = T.yc[j0];
-  c.pol = 0.0; c.vrot = 0.0; c.dvol0 = 1.0; c.sinpol = 0.0; c.cospol = 0.0;
+  c.pol = 0.0; c.vrot = 0.0; c.dvol0 = 1.0; c.sinpol = 0.0; c.cospol = 0.0; c.sinfz = 0.0; c.cosfz = 0.0;
   // the pencil's planet angle factor at the start of the step, once
   if (n == 0) S.cf0 = ph.plnt ? planet_cosfac(c.azi, st.pl, 0.0) : 0.0;
   double rad_cyl = 1.0;
@@ -437,6 +437,8 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
     c.pol = zc;
     c.sinpol = T.szc[kr + NPAD];      // sin, cos of the layer's centre angle
     c.cospol = T.czc[kr + NPAD];
+    c.sinfz = T.szf[kr + NPAD];       // and of its left face angle
+    c.cosfz = T.czf[kr + NPAD];
     c.dvol0 = zvol * rad;
     S.xa0[n] = za;
     S.dx0[n] = dz;
@@ -560,6 +562,8 @@ __global__ void k_tables(Tables T, Phys ph, int ndim, double kill_rin, double ki
     // sin, cos of every polar layer's centre angle (ghost layers included)
     const_cast<double *>(T.szc)[t] = sin(T.zc[t]);
     const_cast<double *>(T.czc)[t] = cos(T.zc[t]);
+    const_cast<double *>(T.szf)[t] = sin(T.z[t]);
+    const_cast<double *>(T.czf)[t] = cos(T.z[t]);
   }
   int k = t / T.nrg, row = t % T.nrg;
   double rad = T.rxc[row];

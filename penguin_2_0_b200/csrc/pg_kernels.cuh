@@ -36,6 +36,7 @@ struct Tables {
   const double *y, *dy, *yvol, *yc;             // [nphi]
   const double *z, *dz, *zvol, *zc;             // [nk + 12]: 6 ghost layers each side
   const double *szc, *czc;                      // [nk + 12]: sin(zc), cos(zc) (k_tables)
+  const double *szf, *czf;                      // [nk + 12]: sin(z), cos(z) of the layer faces
   const double *val_r, *val_u, *val_v;          // [nk*nrg] damping / FARGO targets
   const double *damp_g, *damp_pw;               // [nk*nrg] zone factor, r^-1.5
   const double *tg;                             // [6*nr*4] theta ghost state (udr): r,p,u,v

@@ -42,6 +42,7 @@ struct ChunkShm32 {
   float q[NT + 2], dx[NT + 2], umid[NT + 2], pmid[NT + 2], tmp1[NT + 2], dl[NT + 2];
   double L[NT + 2], Lal[NT + 2], Lda[NT + 2], La6[NT + 2], Lflux[NT + 2], xa0[NT + 2];
   double Rd[NT + 2], dld[NT + 2];   // FP64 Lagrangian density and face displacements
+  double cf0;   // cos(phi - phi_planet) at the start of the step (radial, polar pencils)
 };
 
 struct CellIn32 {
@@ -49,7 +50,10 @@ struct CellIn32 {
   double omres;   // azimuthal sweep: v_bg / r_cyl - v_rot - FrRot (FP64)
   double sig;     // this cell's Sigma in FP64 (S_bg + dS)
   double dx0;     // this cell's Eulerian width in FP64
-  double sinpol;  // sin(pol) for the radial and azimuthal sweeps in 3D
+  double sinpol;  // sin(pol) in 3D (per-layer table)
+  double cospol;  // cos(pol) (polar sweep)
+  double sinfz;   // sin, cos of the left face angle (polar sweep)
+  double cosfz;
 };
 
 __device__ __forceinline__ float min3f(float A, float B, float C) {
@@ -162,9 +166,9 @@ __device__ __forceinline__ double face_force32(int n, double hdt, const CellIn32
     if (!SPH) return ph.plnt ? grav_azi_cyl(c.rad, azi, c.pol, pl, hdt) : 0.0;
     return ph.plnt ? grav_azi_sph_s(c.rad, azi, c.sinpol, pl, hdt) : 0.0;
   } else {
-    double pol = xa0f;
+    // the face angle xa0f is the layer's face: sin, cos from the table
     double azi = c.azi + hdt * c.vrot;
-    const double sp = sin(pol), cp = cos(pol);
+    const double sp = c.sinfz, cp = c.cosfz;
     double grav = ph.plnt ? grav_pol_sph_s(c.rad, azi, sp, cp, pl, hdt) : 0.0;
     double rc = c.rad * sp;
     double lf = 0.5 * (Lv[n] + Lv[n - 1]);
@@ -172,18 +176,25 @@ __device__ __forceinline__ double face_force32(int n, double hdt, const CellIn32
   }
 }
 
-template <int AXIS, bool SPH>
+// CF0: cos(azi - p.y) given as cf0 (the dt = 0 force of a radial or polar
+// pencil); the polar form takes sin and cos of its angle as sp, cp.
+template <int AXIS, bool SPH, bool CF0 = false>
 __device__ __forceinline__ double centre_force32(int n, double dt, double rad, double azi, double pol,
                                                  double sinpol, const double *Lv, const float *wv,
-                                                 const Body &pl, const Phys &ph) {
+                                                 const Body &pl, const Phys &ph, double cf0 = 0.0,
+                                                 double sp = 0.0, double cp = 0.0) {
   if (AXIS == 0) {
     double grav;
     if (!SPH) {
-      if (ph.plnt) { grav = grav_rad_cyl(rad, azi, pol, pl, dt); grav += -1.0 / rad / rad; }
+      if (ph.plnt) {
+        grav = CF0 ? grav_rad_cyl_cf(rad, cf0, pol, pl) : grav_rad_cyl(rad, azi, pol, pl, dt);
+        grav += -1.0 / rad / rad;
+      }
       else { double dis = sqrt(rad * rad + pol * pol); grav = -rad / dis / dis / dis; }
       return grav + Lv[n] * Lv[n] / rad / rad / rad;
     } else {
-      grav = ph.plnt ? grav_rad_sph_s(rad, azi, sinpol, pl, dt) : -1.0 / rad / rad;
+      if (ph.plnt) grav = CF0 ? grav_rad_sph_cf(rad, cf0, sinpol, pl) : grav_rad_sph_s(rad, azi, sinpol, pl, dt);
+      else grav = -1.0 / rad / rad;
       double w = wv[n];
       double rs = rad * sinpol;
       return grav + w * w / rad / rad / rad + Lv[n] * Lv[n] / rad / (rs * rs);
@@ -192,8 +203,9 @@ __device__ __forceinline__ double centre_force32(int n, double dt, double rad, d
     if (!SPH) return ph.plnt ? grav_azi_cyl(rad, azi, pol, pl, dt) : 0.0;
     return ph.plnt ? grav_azi_sph_s(rad, azi, sinpol, pl, dt) : 0.0;
   } else {
-    const double sp = sin(pol), cp = cos(pol);
-    double grav = ph.plnt ? grav_pol_sph_s(rad, azi, sp, cp, pl, dt) : 0.0;
+    (void)pol;
+    double grav = 0.0;
+    if (ph.plnt) grav = CF0 ? grav_pol_sph_cf(rad, cf0, sp, cp, pl) : grav_pol_sph_s(rad, azi, sp, cp, pl, dt);
     double rc = rad * sp;
     return grav + (Lv[n] * Lv[n] * cp) / rc / rc / rc;
   }
@@ -310,23 +322,30 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
     xa = xa0n + S.dld[n];
   }
   __syncthreads();
+  double sxcl = 0.0;   // polar: sin of the new centre angle, reused by the volume
   if (n >= 3 && n < nmax - 3) {
     double xcl = xa + 0.5 * dxld;
     double a1, a2;
     if (AXIS == 0) {
-      a1 = centre_force32<0, SPH>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S.L, S.w, pl, ph);
+      a1 = centre_force32<0, SPH, true>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S.L, S.w, pl, ph, S.cf0);
       a2 = centre_force32<0, SPH>(n, dt, xcl, c.azi + dt * c.vrot, c.pol, c.sinpol, S.L, S.w, pl, ph);
     } else if (AXIS == 1) {
       a1 = centre_force32<1, SPH>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S.L, S.v, pl, ph);
       a2 = centre_force32<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, c.sinpol, S.L, S.v, pl, ph);
     } else {
-      a1 = centre_force32<2, SPH>(n, 0.0, c.rad, c.azi, c.pol, 0.0, S.L, S.v, pl, ph);
-      a2 = centre_force32<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, 0.0, S.L, S.v, pl, ph);
+      a1 = centre_force32<2, SPH, true>(n, 0.0, c.rad, c.azi, c.pol, 0.0, S.L, S.v, pl, ph, S.cf0, c.sinpol,
+                                        c.cospol);
+      sxcl = sin(xcl);
+      a2 = centre_force32<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, 0.0, S.L, S.v, pl, ph, 0.0, sxcl,
+                                  cos(xcl));
     }
     fto1 = (float)a1;
     fto2 = (float)a2;
   }
   __syncthreads();
+  // polar: the volume factor's two sines, reused by the remap's overlap volume
+  double sA = 0.0, sB = 0.0;
+  bool haveS = false;
   if (n >= 3 && n < nmax - 2) {
     // as in the reference, the last cell of this range keeps xa = xa0
     // (evolve.cu:36-44 sets xa for n < nmax-3 only)
@@ -341,9 +360,15 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
     } else if (AXIS == 1) {
       dvol = dxn * c.rad; vfac[n] = 1.0f;
     } else {
-      dvol = 2.0 * sin(xa + 0.5 * dxn) * sin(0.5 * dxn) * c.rad;
+      const double sc = (n < nmax - 3) ? sxcl : sin(xa + 0.5 * dxn);
+      dvol = 2.0 * sc * sin(0.5 * dxn) * c.rad;
       if (d == 0.0) vfac[n] = (float)sin(xa);
-      else vfac[n] = (float)(2.0 * sin(xa0n + 0.5 * d) * sin(0.5 * d) / d);
+      else {
+        sA = sin(xa0n + 0.5 * d);
+        sB = sin(0.5 * d);
+        haveS = (n < nmax - 3);
+        vfac[n] = (float)(2.0 * sA * sB / d);
+      }
     }
   }
   __syncthreads();
@@ -370,7 +395,8 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
   } else if (AXIS == 1) {
     lvol = dd * c.rad;
   } else {
-    lvol = 2.0 * sin(xa0n + 0.5 * dd) * sin(0.5 * dd) * c.rad;
+    if (haveS) lvol = 2.0 * sA * sB * c.rad;
+    else lvol = 2.0 * sin(xa0n + 0.5 * dd) * sin(0.5 * dd) * c.rad;
   }
   const bool delC = (dd >= 0.0);
   float *flux = S.dx;

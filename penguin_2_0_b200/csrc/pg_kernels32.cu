@@ -110,8 +110,10 @@ __device__ __forceinline__ void sweep_x32_body(ChunkShm32<NT> &S, int n, bool st
     sbg = T.sbg[rk];
     c.azi = T.yc[j0];
     c.pol = THREED ? T.zc[k + NPAD] : 0.0;
-    c.sinpol = THREED ? sin(c.pol) : 0.0;
+    c.sinpol = THREED ? T.szc[k + NPAD] : 0.0;
     c.dvol0 = T.rxvol[row];
+    // the pencil's planet angle factor at the start of the step, once
+    if (n == 0) S.cf0 = ph.plnt ? planet_cosfac(c.azi, st.pl, 0.0) : 0.0;
     c.vrot = T.res_v[rk] / rad_cyl;
     S.xa0[n] = T.rx[row];
     S.dx0[n] = (float)T.rdx[row];
@@ -276,7 +278,7 @@ __device__ __forceinline__ void sweep_y32_body(ChunkShm32<NT> &S, double *red, c
     CellIn32 c;
     c.rad = rad_cyl;
     c.pol = THREED ? T.zc[k + NPAD] : 0.0;
-    c.sinpol = THREED ? sin(c.pol) : 0.0;
+    c.sinpol = THREED ? T.szc[k + NPAD] : 0.0;
     c.vrot = T.res_v[rk] / rad_cyl;
     c.omres = vbg / rad_cyl - c.vrot - st.frrot;
     c.azi = 0.0; c.dvol0 = 1.0; c.sig = 1.0; c.dx0 = 0.0;
@@ -386,13 +388,17 @@ __device__ __forceinline__ void sweep_z32_body(ChunkShm32<NT> &S, int n, bool st
   const int kr = n - NPAD + REAL * l;
   const double rad = T.rxc[row];
   CellIn32 c{rad, T.yc[j0], 0.0, 0.0, 1.0, 0.0, 1.0};
+  // the pencil's planet angle factor at the start of the step, once
+  if (n == 0) S.cf0 = ph.plnt ? planet_cosfac(c.azi, st.pl, 0.0) : 0.0;
   double rad_cyl = 1.0, vbg = 0.0, sbg = 0.0;
   if (act) {
     double za, dz, zc, zvol, L;
     float r, p, u, w;
     int kz = kr + NPAD;
     za = T.z[kz]; dz = T.dz[kz]; zc = T.zc[kz]; zvol = T.zvol[kz];
-    rad_cyl = rad * sin(zc);
+    // sin, cos of the layer's centre and face angles from the tables
+    c.sinpol = T.szc[kz]; c.cospol = T.czc[kz]; c.sinfz = T.szf[kz]; c.cosfz = T.czf[kz];
+    rad_cyl = rad * c.sinpol;
     if (kr < 0) {
       const double *g = T.tg + ((size_t)kz * T.nr + i) * 4;
       c.sig = g[0];

@@ -37,12 +37,17 @@ constexpr float kSmallrF = 1.0e-15f;
 constexpr float kFourthdF = 1.3333333333333333f;
 
 template <int NT>
-struct ChunkShm32 {
+struct ChunkShm32Data {
   float r[NT + 2], p[NT + 2], u[NT + 2], v[NT + 2], w[NT + 2], dx0[NT + 2];
   float q[NT + 2], dx[NT + 2], umid[NT + 2], pmid[NT + 2], tmp1[NT + 2], dl[NT + 2];
   double L[NT + 2], Lal[NT + 2], Lda[NT + 2], La6[NT + 2], Lflux[NT + 2], xa0[NT + 2];
   double Rd[NT + 2], dld[NT + 2];   // FP64 Lagrangian density and face displacements
   double cf0;   // cos(phi - phi_planet) at the start of the step (radial, polar pencils)
+};
+// padded to 32 mod 128 bytes: conflict-free banks for 4 packed pencils
+template <int NT>
+struct ChunkShm32 : ChunkShm32Data<NT> {
+  char pad_[shm_pad_bytes((int)sizeof(ChunkShm32Data<NT>))];
 };
 
 struct CellIn32 {

@@ -100,12 +100,23 @@ struct Par { double c0, c1, c2, c3, c4; };
 // the q remap is dead in EOS 0 and 1.  NT is the CTA size: 128 for full
 // chunks, 64 or 32 for a short last chunk (lim <= NT).
 template <int NT>
-struct ChunkShmT {
+struct ChunkShmData {
   double r[NT + 2], p[NT + 2], u[NT + 2], v[NT + 2], w[NT + 2], xa0[NT + 2], dx0[NT + 2];
   double q[NT + 2], dx[NT + 2], umid[NT + 2], pmid[NT + 2], tmp1[NT + 2];
   // cos(phi - phi_planet) at the start of the step: one value for a radial
   // or polar pencil, whose cells share the azimuth phi (written by cell 0)
   double cf0;
+};
+
+// Bytes that bring a per-pencil shared block to 32 mod 128.  Kernels that
+// pack 4 pencils per CTA (thread t on cell t/4 of pencil t%4) then place the
+// four pencils' 32-byte pieces of a half-warp's 64-bit access (or a warp's
+// 32-bit one) in four different bank groups, without bank conflicts.
+constexpr int shm_pad_bytes(int size) { return ((32 - size % 128) + 256) % 128 == 0 ? 128 : ((32 - size % 128) + 256) % 128; }
+
+template <int NT>
+struct ChunkShmT : ChunkShmData<NT> {
+  char pad_[shm_pad_bytes((int)sizeof(ChunkShmData<NT>))];
 };
 
 // ---- star + planet gravity, forces.cu:23-182 (non-barycentric frame) ------

@@ -17,7 +17,8 @@
 //     full rings in the dump layout.
 //
 // usage: penguin_ref <ic_dump> <nsteps> <outdir> <steps-to-save, comma separated> [nodiag]
-// (nodiag: skip the mass/torque reductions, for timing the sweeps)
+// (nodiag: skip the mass/torque reductions, for timing the sweeps; the token
+// "end" in the list saves the state after the last step as state_final.bin)
 #include <unistd.h>
 #include <cstdio>
 #include <cstdlib>
@@ -85,11 +86,13 @@ int main(int argc, char **argv)
   int nsteps = atoi(argv[2]);
   string outdir = argv[3];
   bool keep[100000] = {false};
+  bool keep_end = false;
   {
     string ks = argv[4];
     stringstream ss(ks);
     string tok;
     while (getline(ss, tok, ',')) {
+      if (tok == "end") { keep_end = true; continue; }
       int v = atoi(tok.c_str());
       if (v > 0 && v < 100000) keep[v] = true;
     }
@@ -212,6 +215,12 @@ int main(int argc, char **argv)
     }
   }
   fclose(hf);
+  if (keep_end) {
+    CudaSafeCall(cudaMemcpy(set[0].h_rings, set[0].rings, set[0].memsize, cudaMemcpyDeviceToHost));
+    ofstream of((outdir + "/state_final.bin").c_str(), ios::out | ios::binary);
+    save_cells(of, set);
+    of.close();
+  }
   printf("{\"steps\": %d, \"cells\": %d, \"sweep_ms_total\": %.6f}\n", ncycle, imax * jmax * kmax, sweep_ms);
   CudaSafeCall(cudaFree(set[0].rings));
   CudaSafeCall(cudaFreeHost(set[0].h_rings));

@@ -13,6 +13,7 @@ Three stages:
          the reference's storage order.
 
 usage: python tests/golden/make_golden.py [--only=case,...] build | run <rawdir> | pack <rawdir> [outdir [fulldir]]
+                                          | run_long <rawdir> | pack_long <rawdir> [outdir]
 (--only restricts build, run and pack to the named cases)
 """
 import ctypes as C
@@ -55,6 +56,15 @@ CASES = {
 }
 
 
+# Whole runs to the end time (the workload's 10 orbits): name -> (base
+# workload, overrides, step limit).  The fixture keeps the history of every
+# step and the full final state.  252 x 780 is the warp-aligned size nearest
+# the 256 x 768 disk (see above).
+LONG_CASES = {
+    "g252x780_10orbits": (0, dict(imax=252, jmax=780), 6000),
+}
+
+
 # Timing builds of the reference (sweeps only, no diagnostics reductions):
 # name -> (base workload, overrides, nsteps).  Warp-aligned sizes near the
 # 256x768 and 1024x3072 disks.
@@ -66,7 +76,7 @@ PERF_CASES = {
 
 def params_for(case):
     from penguin_2_0_b200 import _lib
-    base, over, *_ = CASES[case] if case in CASES else PERF_CASES[case]
+    base, over, *_ = CASES[case] if case in CASES else (LONG_CASES[case] if case in LONG_CASES else PERF_CASES[case])
     p = _lib.pg_params()
     st = _lib.lib().pg_config_params(base, C.byref(p))
     assert st == 0
@@ -87,7 +97,7 @@ def _cases(names):
 
 
 def cmd_build():
-    for case in _cases(list(CASES) + list(PERF_CASES)):
+    for case in _cases(list(CASES) + list(PERF_CASES) + list(LONG_CASES)):
         p = params_for(case)
         d = os.path.join(ROOT, "oracle", "_ref", case)
         os.makedirs(d, exist_ok=True)
@@ -145,6 +155,71 @@ def cmd_run(rawdir):
         print(case, f"{time.time() - t0:.1f}s", r.stdout.strip(), flush=True)
 
 
+PERTURB_CELL = (126, 390)   # (ring, j) of the 1-ulp change of Sigma in the perturbed run
+
+
+def cmd_run_long(rawdir):
+    """Runs each long case twice: from the seeded dump, and from the same dump
+    with Sigma of one cell (PERTURB_CELL, a ring at the planet's radius)
+    moved up by one ulp.  The second run measures how far the reference's
+    own result moves under a rounding-sized change of its input."""
+    from penguin_2_0_b200 import _lib
+    L = _lib.lib()
+    for case in _cases(LONG_CASES):
+        _, _, limit = LONG_CASES[case]
+        p = params_for(case)
+        out = os.path.join(rawdir, case)
+        pert = os.path.join(out, "pert")
+        os.makedirs(pert, exist_ok=True)
+        ic = os.path.join(out, "ic.bin")
+        assert L.pg_write_ic(C.byref(p), ic.encode()) == 0
+        raw = np.fromfile(ic, dtype=np.uint8)
+        ring, j = PERTURB_CELL
+        off = ring * (72 * p.jmax + 96) + 8 * j
+        x = raw[off:off + 8].copy().view(np.float64)
+        raw[off:off + 8] = np.nextafter(x, np.inf).view(np.uint8)
+        icp = os.path.join(out, "ic_pert.bin")
+        raw.tofile(icp)
+        exe = os.path.join(ROOT, "oracle", "_ref", case, "penguin_ref")
+        for src, dst in ((ic, out), (icp, pert)):
+            t0 = time.time()
+            r = subprocess.run(["timeout", "-k", "10", "600", exe, src, str(limit), dst, "end"],
+                               capture_output=True, text=True)
+            open(os.path.join(dst, "stdout.txt"), "w").write(r.stdout + r.stderr)
+            if r.returncode != 0:
+                raise SystemExit(f"{case}: reference exited {r.returncode}: {r.stderr[-400:]}")
+            print(case, os.path.basename(src), f"{time.time() - t0:.1f}s", r.stdout.strip(), flush=True)
+        os.remove(ic)
+        os.remove(icp)
+
+
+def _hist(path):
+    rows = [ln.split() for ln in open(path)]
+    return np.array([[float.fromhex(x) for x in r[1:]] for r in rows])
+
+
+def long_errors(f_r, f_u, f_v, ref):
+    """Relative L1 of Sigma, of v_r (to the L1 of v_phi) and of v_phi; ref is
+    [ring, (Sigma, v_r, v_phi), jmax]."""
+    l1 = lambda a, b, sc: float(np.sum(np.abs(a - b)) / np.sum(np.abs(sc)))
+    return (l1(f_r, ref[:, 0], ref[:, 0]), l1(f_u, ref[:, 1], ref[:, 2]), l1(f_v, ref[:, 2], ref[:, 2]))
+
+
+def cmd_pack_long(rawdir, outdir=HERE):
+    for case in _cases(LONG_CASES):
+        p = params_for(case)
+        src = os.path.join(rawdir, case)
+        hist = _hist(os.path.join(src, "hist.txt"))
+        hist_p = _hist(os.path.join(src, "pert", "hist.txt"))
+        f, rot_j = read_rings(os.path.join(src, "state_final.bin"), p)
+        fp, _ = read_rings(os.path.join(src, "pert", "state_final.bin"), p)
+        ref = f[:, [0, 2, 3], :].copy()
+        pert = long_errors(fp[:, 0], fp[:, 2], fp[:, 3], ref)
+        np.savez_compressed(os.path.join(outdir, f"{case}.npz"), hist=hist, fields=ref, rot_j=rot_j,
+                            hist_pert=hist_p, pert_l1=np.array(pert), perturb_cell=np.array(PERTURB_CELL))
+        print("packed", case, hist.shape[0], "steps; 1-ulp sensitivity L1 (Sigma, v_r, v_phi):", pert)
+
+
 def read_rings(path, p):
     jmax = p.jmax
     n = p.imax * p.kmax
@@ -198,5 +273,9 @@ if __name__ == "__main__":
         cmd_perf(sys.argv[2])
     elif what == "pack":
         cmd_pack(sys.argv[2], *(sys.argv[3:5]))
+    elif what == "run_long":
+        cmd_run_long(sys.argv[2])
+    elif what == "pack_long":
+        cmd_pack_long(sys.argv[2], *(sys.argv[3:4]))
     else:
         raise SystemExit(__doc__)

@@ -53,16 +53,16 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     # name: (config index, overrides, description)
-    "cfg0": (0, {}, "2D r-phi disk 256x768 FP64, planet q=1e-3, FARGO, damping (configs[0])"),
-    "cfg1": (1, {}, "3D spherical disk 128x1024x32 FP64, reflecting midplane (configs[1])"),
+    "cfg0": (0, {}, "2D r-phi disk 256x768 FP64, planet q=1e-3, FARGO, damping"),
+    "cfg1": (1, {}, "3D spherical disk 128x1024x32 FP64, reflecting midplane"),
     "cfg2": (2, {}, "2D r-phi disk 1024x3072 FP32 planes (precision form), same disk and planet"),
     "cfg2_fp64": (2, {"precision": 0}, "2D r-phi disk 1024x3072 FP64, same disk and planet"),
     "cfg0_fp32": (0, {"precision": 1}, "2D r-phi disk 256x768 FP32 planes, planet q=1e-3"),
     "big": (0, {"imax": 4096, "jmax": 12288}, "2D r-phi disk 4096x12288 FP64, same disk"),
     "prof": (0, {"imax": 2048, "jmax": 6144}, "2D r-phi disk 2048x6144 FP64 (profiling case, > L2)"),
     "prof32": (0, {"imax": 2048, "jmax": 6144, "precision": 1}, "2D r-phi disk 2048x6144 FP32 planes (> L2)"),
-    "ens": (None, {}, "batched ensemble of 64 2D disks (configs[3])"),
-    "serve": (None, {}, "serving stream (configs[4] sample)"),
+    "ens": (None, {}, "batched ensemble of 64 2D disks"),
+    "serve": (None, {}, "serving stream (sample)"),
 }
 
 
@@ -287,7 +287,7 @@ def bench_ensemble(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": f"mixed: f32 planes for {n32} disks, f64 for {n - n32}",
         "data": "synthetic seeded disks (no public dataset)",
-        "config": {"workload": f"batched ensemble of {n} 2D disks, {orbits:g} orbits each (configs[3])",
+        "config": {"workload": f"batched ensemble of {n} 2D disks, {orbits:g} orbits each",
                    "cells": sum(E.disk_cells(p) for p in ps), "fp32_disks": n32,
                    "policy": f"FP32 planes when q/h^3 <= {E.THERMAL_MASS_FP32}",
                    "l2": "working set larger than L2", "tuned_shape": None},
@@ -341,7 +341,7 @@ def bench_serve(args):
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": f"mixed: f32 planes for {sum(p.precision for p in reqs)} of {n} requests",
         "data": "synthetic seeded request stream (no public dataset)",
-        "config": {"workload": f"serving {n} requests (sample of configs[4]'s 2000), orbits "
+        "config": {"workload": f"serving {n} requests (sample of the 2000-request stream), orbits "
                                f"{5 * scale:g}-{50 * scale:g} (x{scale:g} of 5-50), 10% 3D",
                    "arrivals": f"Poisson, {rate:.3f}/s = 1.5 x measured capacity {capacity:.3f}/s",
                    "hbm_budget_gb": 150, "max_slots": slots, "chunk": args.chunk},

@@ -1,11 +1,11 @@
 """Multi-GPU use of the hydro step: independent replicas, one per rank.
 
-The path has no exchange step at the north-star sizes (one disk fits one GPU),
+The path has no exchange step at the workload sizes (one disk fits one GPU),
 so N GPUs advance N independent disks (ensemble members / served runs); the
 only collective is a max over ranks of the timed region, which is how the
 whole-job throughput is reported.  No halo exchange is built (the
 reference's radial slab split, main.cu:145-188 / ppm.cu:326-355, is a
-single-run decomposition the north star does not ask for).
+single-run decomposition for disks larger than one GPU's memory).
 """
 from __future__ import annotations
 

@@ -30,7 +30,8 @@ seeded dump is loaded from pinned host memory (pg_load_rings), pg_clock_reset
 and pg_advance_graph (the ABI's replacement of main.cu's loop) run the steps,
 every step's diagnostics row (dt, mass, torque, ...) is read back (pg_history)
 and the final dump is saved to pinned host memory, all inside the timed
-region.  e2e_host_loop times the reference's per-call sequence instead
+region; the job runs three times and the median is reported.
+e2e_host_loop times the reference's per-call sequence instead
 (pg_get_dt, pg_index_shift, pg_sweep2d/3d, pg_damp, pg_reduce from a Python
 loop with main.cu's host syncs: dt, planet and FrRot to the device, dt, mass
 and torque back every step).
@@ -50,6 +51,8 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+
+E2E_JOBS = 3      # e2e jobs timed; the median is reported
 
 WORKLOADS = {
     # name: (config index, overrides, description)
@@ -488,16 +491,21 @@ def main():
     run2.clock_reset(0)
     run2.advance(args.chunk, graph_chunk=args.chunk)     # graph capture outside the timed job
     torch.cuda.synchronize()
-    _barrier(dist)
-    t0 = time.perf_counter()
-    run2.load_from(pin_in.data_ptr(), dump_bytes)
-    run2.clock_reset(0)
-    done = run2.advance(e2e_steps, graph_chunk=args.chunk)
-    hist = run2.history(max_rows=e2e_steps)
-    run2.save_to(pin_out.data_ptr(), dump_bytes)
-    torch.cuda.synchronize()
-    e2e_el = _max_over_ranks(dist, time.perf_counter() - t0)
-    assert done == e2e_steps and hist.shape[0] == e2e_steps, (done, hist.shape)
+    # the job runs E2E_JOBS times; the median job time is reported (one job
+    # is ~0.5 s, short enough for a one-off host or bus stall to dominate it)
+    jobs = []
+    for _ in range(E2E_JOBS):
+        _barrier(dist)
+        t0 = time.perf_counter()
+        run2.load_from(pin_in.data_ptr(), dump_bytes)
+        run2.clock_reset(0)
+        done = run2.advance(e2e_steps, graph_chunk=args.chunk)
+        hist = run2.history(max_rows=e2e_steps)
+        run2.save_to(pin_out.data_ptr(), dump_bytes)
+        torch.cuda.synchronize()
+        jobs.append(_max_over_ranks(dist, time.perf_counter() - t0))
+        assert done == e2e_steps and hist.shape[0] == e2e_steps, (done, hist.shape)
+    e2e_el = sorted(jobs)[len(jobs) // 2]
     e2e_value = cells * e2e_steps * ws / e2e_el
     run2.close()
 
@@ -510,13 +518,16 @@ def main():
         if p.plnt_flag:
             pg.GPU_output_reduction(run3, planet, 0.0, 9)
 
-    _barrier(dist)
-    t0 = time.perf_counter()
-    run3.load_from(pin_in.data_ptr(), dump_bytes)
-    run3.kernel_loop(e2e_steps, record=rec)
-    run3.save_to(pin_out.data_ptr(), dump_bytes)
-    torch.cuda.synchronize()
-    hl_el = _max_over_ranks(dist, time.perf_counter() - t0)
+    hl_jobs = []
+    for _ in range(E2E_JOBS):
+        _barrier(dist)
+        t0 = time.perf_counter()
+        run3.load_from(pin_in.data_ptr(), dump_bytes)
+        run3.kernel_loop(e2e_steps, record=rec)
+        run3.save_to(pin_out.data_ptr(), dump_bytes)
+        torch.cuda.synchronize()
+        hl_jobs.append(_max_over_ranks(dist, time.perf_counter() - t0))
+    hl_el = sorted(hl_jobs)[len(hl_jobs) // 2]
     hl_value = cells * e2e_steps * ws / hl_el
     run3.close()
 
@@ -545,13 +556,13 @@ def main():
             "e2e": {"value": e2e_value, "unit": "zone-updates/s",
                     "h2d_bytes_per_step": dump_bytes / e2e_steps,
                     "d2h_bytes_per_step": (dump_bytes + 8 * 11 * e2e_steps) / e2e_steps,
-                    "steps": e2e_steps,
+                    "steps": e2e_steps, "jobs_s": [round(j, 4) for j in jobs], "reported": "median job",
                     "path": "pg_load_rings from pinned host memory, pg_clock_reset + pg_advance_graph "
                             "(device-resident loop, nprin 1), pg_history rows, pg_save_rings to pinned host memory"},
             "e2e_host_loop": {"value": hl_value, "unit": "zone-updates/s",
                               "h2d_bytes_per_step": (dump_bytes + (64 + 16) * e2e_steps) / e2e_steps,
                               "d2h_bytes_per_step": (dump_bytes + (8 + 8 + 8) * e2e_steps) / e2e_steps,
-                              "steps": e2e_steps,
+                              "steps": e2e_steps, "jobs_s": [round(j, 4) for j in hl_jobs],
                               "path": "pg_load_rings from pinned host memory, host loop (Python) over pg_get_dt/"
                                       "pg_index_shift/pg_sweep2d|3d/pg_damp/pg_reduce with main.cu's syncs, "
                                       "pg_save_rings to pinned host memory"},

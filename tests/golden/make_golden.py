@@ -53,6 +53,10 @@ CASES = {
     # isentropic EOS 1, gam 1.4: the Newton Riemann solver (riemann.cu:75-111)
     # and p = cs2 Sigma^gam / gam at every store; planet, viscosity, damping
     "g136x200_eos1": (0, dict(imax=136, jmax=200, EOS=1, gam=1.4), 8, (1, 3, 8)),
+    # FARGO_flag 2: rings shift at the solid-body rate (1 - FrRot) r; with the
+    # frame rotating at the orbit of a planet at R_p = 0.3 (FrRot = 6.1) every
+    # ring moves by whole cells each step
+    "g136x136_fargo2": (0, dict(imax=136, jmax=136, FARGO_flag=2, R_p=0.3), 8, (1, 8)),
 }
 
 

@@ -42,7 +42,7 @@ def test_host_loop_matches_reference_build(gpu, case):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["g136x136", "g252x780", "g136x200_eos1"])
+@pytest.mark.parametrize("case", ["g136x136", "g252x780", "g136x200_eos1", "g136x136_fargo2"])
 def test_fused_loop_matches_reference_build(gpu, case):
     _, _, nsteps, keep = CASES[case]
     p = params_for(case)

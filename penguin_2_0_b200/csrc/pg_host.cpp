@@ -92,9 +92,14 @@ double Profile::vol(double xa, double dx, int axis) const {
   return v;
 }
 
-// ---- grid generator grid.cu:67-221 -----------------------------------------
-static int make_grid(int nz, double lo, double hi, int lg, double dmin, double dmax,
+// ---- grid generator grid.cu:66-221 -----------------------------------------
+// Type 4 (refined toward the centre) takes the radial limits dx_min/dx_max
+// and type 6 (refined toward the upper edge) the polar limits dz_min/dz_max
+// whichever axis it builds, as the reference's global constants do.
+static int make_grid(const pg_params &P, int nz, double lo, double hi, int lg,
                      std::vector<double> &xa, std::vector<double> &xc, std::vector<double> &dx) {
+  const double dmin = (lg == 4) ? P.dx_min : P.dz_min;
+  const double dmax = (lg == 4) ? P.dx_max : P.dz_max;
   xa.assign(nz, 0.0); xc.assign(nz, 0.0); dx.assign(nz, 0.0);
   if (lg == 0) {
     double f = (hi - lo) / (double)nz;
@@ -345,9 +350,9 @@ int build_ic(const pg_params *p, void *buf, size_t bytes, std::string &why) {
   if (!buf || bytes != rbytes * (size_t)P.imax * P.kmax) { why = "ring buffer size mismatch"; return PG_ERR_ARG; }
   Profile pf{P};
   std::vector<double> zxa, zxc, zdx, zya, zyc, zdy, zza, zzc, zdz;
-  if (make_grid(P.imax, P.xmin, P.xmax, P.grspx, P.dx_min, P.dx_max, zxa, zxc, zdx) ||
-      make_grid(P.jmax, P.ymin, P.ymax, P.grspy, P.dy_min, P.dy_max, zya, zyc, zdy) ||
-      make_grid(P.kmax, P.zmin, P.zmax, P.grspz, P.dz_min, P.dz_max, zza, zzc, zdz)) {
+  if (make_grid(P, P.imax, P.xmin, P.xmax, P.grspx, zxa, zxc, zdx) ||
+      make_grid(P, P.jmax, P.ymin, P.ymax, P.grspy, zya, zyc, zdy) ||
+      make_grid(P, P.kmax, P.zmin, P.zmax, P.grspz, zza, zzc, zdz)) {
     why = "unsupported grid type"; return PG_ERR_PARAMS;
   }
   std::vector<SymDisk> val;

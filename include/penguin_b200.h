@@ -120,6 +120,18 @@ size_t pg_ring_bytes(int jmax);
 int pg_write_ic(const pg_params *p, const char *path);
 int pg_build_ic(const pg_params *p, void *rings, size_t bytes);
 
+/* The fixed boundary rings that init_bound (init.cpp:253-543) sets up, on
+ * the grid of *p: per ring PG_BOUNDARY_FIELDS doubles x, dx, xvol, xc, z, dz,
+ * zvol, zc, Sigma, p, v_r, v_phi, v_theta, rot_v.  Order: the 6 x kmax inner
+ * radial rings (ring i + 6 k), the 6 x kmax outer ones, then in 3D the
+ * 6 x imax polar layers below the first layer and the 6 x imax above the
+ * last (layer k + 6 i; the ones above hold what ntop = 3 fixes).  These are
+ * the values the run loads into its ghost rows and polar ghost layers.
+ * *count receives the number of rings; out may be null to ask for it.
+ * Host only.                                                               */
+#define PG_BOUNDARY_FIELDS 14
+int pg_boundary_rings(const pg_params *p, double *out, size_t n_doubles, int *count);
+
 /* Run label of create_label() (output.cu:57-88) into buf.                  */
 int pg_label(const pg_params *p, char *buf, size_t len);
 

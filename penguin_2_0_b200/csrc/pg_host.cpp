@@ -23,16 +23,27 @@ const double kJupiterMass = 0.001;
 const double kMMSN = 0.00019126835;
 
 // ---- disk profile (disk_profile.cu) --------------------------------------
+// pow with the forms the reference's compiler gives it: its exponents are
+// compile-time constants, and pow(x, 0), pow(x, 1), pow(x, -1) and pow(x, 2)
+// are folded to 1, x, 1/x and x*x (exact or correctly rounded, where libm's
+// pow can differ by an ulp); other exponents stay calls.
+static double cpow_c(double x, double y) {
+  if (y == 0.0) return 1.0;
+  if (y == 1.0) return x;
+  if (y == -1.0) return 1.0 / x;
+  if (y == 2.0) return x * x;
+  return std::pow(x, y);
+}
 double Profile::rho(double r) const {                                           // 9-28
   // the 3D isentropic disk's midplane slope is p_alpha 2/(gam + 1)
   double n = (P.EOS != 0 && P.ndim == 3) ? -P.p_alpha * (2.0 / (P.gam + 1.0)) : -P.p_alpha;
-  return std::pow(r, n);
+  return cpow_c(r, n);
 }
-double Profile::cs2(double r) const { return P.sc_h * P.sc_h * std::pow(r, -P.p_beta); }  // 39-42
+double Profile::cs2(double r) const { return P.sc_h * P.sc_h * cpow_c(r, -P.p_beta); }  // 39-42
 double Profile::h(double r) const { return std::sqrt(cs2(r) * r * r * r); }      // 49-52
 double Profile::pres(double r) const {                                          // 54-61
   if (P.EOS == 0) return cs2(r) * rho(r);
-  return cs2(r) * std::pow(rho(r), P.gam) / P.gam;
+  return cs2(r) * cpow_c(rho(r), P.gam) / P.gam;
 }
 double Profile::dP_dr(double r) const {                                          // 63-68
   double p1 = pres(r + 1.27245e-8);
@@ -50,14 +61,14 @@ double Profile::rho(double r, double z) const {                                 
   // (1 - r/sqrt(r^2 + z^2)), continued above z_0 by a decade per h/6
   const double gm = P.gam - 1.0;
   double h = std::sqrt(cs2(r) * r * r * r);
-  double z0 = std::sqrt(2.0 * h * h * std::pow(r, -P.p_alpha * (2.0 / (P.gam + 1.0)) * gm) / gm);
-  if (z < z0) return std::pow(std::pow(rho(r), gm) - (gm / (r * cs2(r))) * (1.0 - r / std::sqrt(r * r + z * z)), 1.0 / gm);
-  double top = std::pow(std::pow(rho(r), gm) - (gm / (r * cs2(r))) * (1.0 - r / std::sqrt(r * r + z0 * z0)), 1.0 / gm);
+  double z0 = std::sqrt(2.0 * h * h * cpow_c(r, -P.p_alpha * (2.0 / (P.gam + 1.0)) * gm) / gm);
+  if (z < z0) return cpow_c(cpow_c(rho(r), gm) - (gm / (r * cs2(r))) * (1.0 - r / std::sqrt(r * r + z * z)), 1.0 / gm);
+  double top = cpow_c(cpow_c(rho(r), gm) - (gm / (r * cs2(r))) * (1.0 - r / std::sqrt(r * r + z0 * z0)), 1.0 / gm);
   return std::pow(10.0, std::log10(top) - 6.0 * (z - z0) / h);
 }
 double Profile::pres(double r, double z) const {                                // 112-118
   if (P.EOS == 0) return cs2(r) * rho(r, z);
-  return cs2(r) * std::pow(rho(r, z), P.gam) / P.gam;
+  return cs2(r) * cpow_c(rho(r, z), P.gam) / P.gam;
 }
 double Profile::dP_s(double r, double pol) const {                               // 128-138
   double dr = 1.27e-7;
@@ -68,7 +79,7 @@ double Profile::dP_s(double r, double pol) const {                              
 }
 double Profile::nu(double r) const {                                             // 149-152
   double vis_nu = P.ss_alpha * P.sc_h * P.sc_h;                                  // global.h:36
-  return vis_nu * std::pow(r, P.p_alpha);
+  return vis_nu * cpow_c(r, P.p_alpha);
 }
 double Profile::viscous_vr(double r) const {                                     // 154-160
   if (P.visc_flag == 1) return -1.5 * nu(r) / r;
@@ -216,6 +227,55 @@ GhostRing make_ghost(const Profile &pf, double x, double dx, double xc, double z
   g.r = rho; g.p = Pr; g.u = pf.viscous_vr(r); g.v = vk; g.w = 0.0;
   g.rot_v = (P.FARGO_flag == 1) ? vk - 1.0 * xc : 0.0;
   return g;
+}
+
+// ---- the fixed boundary rings of init_bound (init.cpp:253-543) ------------
+// Radial ghost rings (lft inside, rgh outside; 6 x kmax each, ring i + 6 k)
+// continue the grid with the edge cell's width; in 3D the polar layers (udr
+// below the first layer, top above the last; 6 x imax each, layer k + 6 i)
+// continue it with the edge layer's width.  Each ring carries the disk
+// profile's axisymmetric state at its centre.  The reference's lft branch for
+// a spherical grid (init.cpp:289-295) forms no density or pressure before
+// using them; here every ring takes the profile's values.
+void boundary_rings(const Profile &pf, const Geometry &g, std::vector<GhostRing> &lft,
+                    std::vector<GhostRing> &rgh, std::vector<GhostRing> &udr, std::vector<GhostRing> &top) {
+  const int pad = 6, nr = pf.P.imax, nk = pf.P.kmax;
+  lft.assign((size_t)pad * nk, GhostRing{});
+  rgh.assign((size_t)pad * nk, GhostRing{});
+  for (int i = 0; i < pad; i++)
+    for (int k = 0; k < nk; k++) {
+      double x = g.zxa[0] - g.zdx[0] * (double)(pad - i), dx = g.zdx[0];
+      lft[i + pad * k] = make_ghost(pf, x, dx, x + 0.5 * dx, g.zza[k], g.zdz[k], g.zzc[k], 0);
+      x = g.zxa[nr - 1] + g.zdx[nr - 1] * (double)(i + 1);
+      dx = g.zdx[nr - 1];
+      rgh[i + pad * k] = make_ghost(pf, x, dx, x + 0.5 * dx, g.zza[k], g.zdz[k], g.zzc[k], 0);
+    }
+  udr.clear();
+  top.clear();
+  if (pf.P.ndim != 3) return;
+  udr.assign((size_t)pad * nr, GhostRing{});
+  top.assign((size_t)pad * nr, GhostRing{});
+  for (int k = 0; k < pad; k++)
+    for (int i = 0; i < nr; i++) {
+      double zl = g.zza[0] - g.zdz[0] * (double)(pad - k), dzl = g.zdz[0];
+      udr[k + pad * i] = make_ghost(pf, g.zxa[i], g.zdx[i], g.zxc[i], zl, dzl, zl + 0.5 * dzl, 1);
+      double zu = g.zza[nk - 1] + g.zdz[nk - 1] * (double)(k + 1), dzu = g.zdz[nk - 1];
+      top[k + pad * i] = make_ghost(pf, g.zxa[i], g.zdx[i], g.zxc[i], zu, dzu, zu + 0.5 * dzu, 1);
+    }
+}
+
+// The grid of a parameter set (init_grid init.cpp:3-57 with get_vol).
+int params_geometry(const pg_params &P, Geometry &g) {
+  Profile pf{P};
+  if (make_grid(P, P.imax, P.xmin, P.xmax, P.grspx, g.zxa, g.zxc, g.zdx) ||
+      make_grid(P, P.jmax, P.ymin, P.ymax, P.grspy, g.zya, g.zyc, g.zdy) ||
+      make_grid(P, P.kmax, P.zmin, P.zmax, P.grspz, g.zza, g.zzc, g.zdz))
+    return PG_ERR_PARAMS;
+  g.xvol.resize(P.imax); g.yvol.resize(P.jmax); g.zvol.resize(P.kmax);
+  for (int i = 0; i < P.imax; i++) g.xvol[i] = pf.vol(g.zxa[i], g.zdx[i], 0);
+  for (int j = 0; j < P.jmax; j++) g.yvol[j] = pf.vol(g.zya[j], g.zdy[j], 1);
+  for (int k = 0; k < P.kmax; k++) g.zvol[k] = pf.vol(g.zza[k], g.zdz[k], 2);
+  return PG_OK;
 }
 
 // ---- dump record layout variable_types.h:67-97 ----------------------------
@@ -381,7 +441,7 @@ int build_ic(const pg_params *p, void *buf, size_t bytes, std::string &why) {
         double U = ic_uniform(P.seed, (uint64_t)m * P.jmax + j);
         double sig = v.r * (1.0 + P.noise_amp * (2.0 * U - 1.0));
         rv.f(0)[j] = sig;
-        rv.f(1)[j] = (P.EOS == 0) ? sig * c2 : c2 * std::pow(sig, P.gam) / P.gam;
+        rv.f(1)[j] = (P.EOS == 0) ? sig * c2 : c2 * cpow_c(sig, P.gam) / P.gam;
         rv.f(2)[j] = 0.0;
         rv.f(3)[j] = v.v;
         rv.f(4)[j] = 0.0;
@@ -461,6 +521,31 @@ int pg_check_params(const pg_params *p) {
 }
 
 size_t pg_ring_bytes(int jmax) { return pg::ring_bytes(jmax); }
+
+int pg_boundary_rings(const pg_params *p, double *out, size_t n_doubles, int *count) {
+  if (!p || !count) return PG_ERR_ARG;
+  std::string why;
+  int st = pg::check_params(p, why);
+  if (st) return st;
+  pg::Geometry g;
+  if ((st = pg::params_geometry(*p, g))) return st;
+  pg::Profile pf{*p};
+  std::vector<pg::GhostRing> lft, rgh, udr, top;
+  pg::boundary_rings(pf, g, lft, rgh, udr, top);
+  const size_t n = lft.size() + rgh.size() + udr.size() + top.size();
+  *count = (int)n;
+  if (!out) return PG_OK;
+  if (n_doubles < n * PG_BOUNDARY_FIELDS) return PG_ERR_ARG;
+  double *o = out;
+  for (const std::vector<pg::GhostRing> *grp : {&lft, &rgh, &udr, &top})
+    for (const pg::GhostRing &r : *grp) {
+      const double rec[PG_BOUNDARY_FIELDS] = {r.x, r.dx, r.xvol, r.xc, r.z, r.dz, r.zvol, r.zc,
+                                              r.r, r.p, r.u, r.v, r.w, r.rot_v};
+      std::memcpy(o, rec, sizeof rec);
+      o += PG_BOUNDARY_FIELDS;
+    }
+  return PG_OK;
+}
 
 int pg_build_ic(const pg_params *p, void *rings, size_t bytes) {
   std::string why;

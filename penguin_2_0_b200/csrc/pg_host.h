@@ -69,6 +69,9 @@ void build_val(const Profile &pf, const std::vector<double> &zxc, const std::vec
                std::vector<SymDisk> &val);
 GhostRing make_ghost(const Profile &pf, double x, double dx, double xc, double z, double dz,
                      double zc, int theta_layer);
+void boundary_rings(const Profile &pf, const Geometry &g, std::vector<GhostRing> &lft,
+                    std::vector<GhostRing> &rgh, std::vector<GhostRing> &udr, std::vector<GhostRing> &top);
+int params_geometry(const pg_params &P, Geometry &g);
 int read_geometry(const pg_params &P, const unsigned char *b, Geometry &g, std::string &why);
 std::string label(const pg_params &P);
 

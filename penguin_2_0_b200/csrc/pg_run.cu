@@ -303,16 +303,8 @@ int pg_load_rings(pg_run *run, const void *rings, size_t bytes) {
   std::vector<int> inc_j(nring, 0), rot_j(nring, 0);
   std::vector<double> z(nz, 0.0), dz(nz, 0.0), zvol(nz, 0.0), zc(nz, 0.0);
   std::vector<double> tg((size_t)2 * NPAD * nr * 4, 0.0);
-  std::vector<pg::GhostRing> lft(NPAD * nk), rgh(NPAD * nk);
-  for (int i = 0; i < NPAD; i++)
-    for (int k = 0; k < nk; k++) {
-      double x = g.zxa[0] - g.zdx[0] * (double)(NPAD - i);
-      double dx = g.zdx[0];
-      lft[i + NPAD * k] = pg::make_ghost(pf, x, dx, x + 0.5 * dx, g.zza[k], g.zdz[k], g.zzc[k], 0);
-      x = g.zxa[nr - 1] + g.zdx[nr - 1] * (double)(i + 1);
-      dx = g.zdx[nr - 1];
-      rgh[i + NPAD * k] = pg::make_ghost(pf, x, dx, x + 0.5 * dx, g.zza[k], g.zdz[k], g.zzc[k], 0);
-    }
+  std::vector<pg::GhostRing> lft, rgh, udr, top;
+  pg::boundary_rings(pf, g, lft, rgh, udr, top);   // init_bound, init.cpp:253-543
   for (int i = 0; i < NPAD; i++) {
     const pg::GhostRing &L = lft[i], &R = rgh[i];
     rx[i] = L.x; rdx[i] = L.dx; rxvol[i] = L.xvol; rxc[i] = L.xc;
@@ -351,13 +343,11 @@ int pg_load_rings(pg_run *run, const void *rings, size_t bytes) {
   if (P.ndim == 3) {
     for (int kk = 0; kk < NPAD; kk++)
       for (int i = 0; i < nr; i++) {
-        pg::GhostRing u = pg::make_ghost(pf, g.zxa[i], g.zdx[i], g.zxc[i], z[kk], dz[kk], zc[kk], 1);
+        const pg::GhostRing &u = udr[kk + NPAD * i];
         double *q = &tg[((size_t)kk * nr + i) * 4];
         q[0] = u.r; q[1] = u.p; q[2] = u.u; q[3] = u.v;
-        size_t qi = NPAD + kk;
-        pg::GhostRing tp = pg::make_ghost(pf, g.zxa[i], g.zdx[i], g.zxc[i], z[nk + NPAD + kk], dz[nk + NPAD + kk],
-                                          zc[nk + NPAD + kk], 1);
-        q = &tg[(qi * nr + i) * 4];
+        const pg::GhostRing &tp = top[kk + NPAD * i];
+        q = &tg[((size_t)(NPAD + kk) * nr + i) * 4];
         q[0] = tp.r; q[1] = tp.p; q[2] = tp.u; q[3] = tp.v;
       }
   }

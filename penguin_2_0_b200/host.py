@@ -79,6 +79,27 @@ def build_ic(p: pg_params) -> bytearray:
     return buf
 
 
+BOUNDARY_FIELDS = ("x", "dx", "xvol", "xc", "z", "dz", "zvol", "zc", "r", "p", "u", "v", "w", "rot_v")
+
+
+def boundary_rings(p: pg_params) -> dict:
+    """The fixed boundary rings of init_bound (init.cpp:253-543) on the grid of
+    p (pg_boundary_rings): {"lft", "rgh", "udr", "top"} -> [rings, 14] arrays
+    with the columns of BOUNDARY_FIELDS; udr and top are empty in 2D."""
+    L = _lib.lib()
+    cnt = C.c_int(0)
+    _check(L.pg_boundary_rings(C.byref(p), None, 0, C.byref(cnt)), what="pg_boundary_rings")
+    nf = len(BOUNDARY_FIELDS)
+    out = np.zeros(cnt.value * nf)
+    _check(L.pg_boundary_rings(C.byref(p), out.ctypes.data_as(C.POINTER(C.c_double)), out.size, C.byref(cnt)),
+           what="pg_boundary_rings")
+    out = out.reshape(cnt.value, nf)
+    nrad = 6 * p.kmax
+    npol = 6 * p.imax if p.ndim == 3 else 0
+    return dict(lft=out[:nrad], rgh=out[nrad:2 * nrad], udr=out[2 * nrad:2 * nrad + npol],
+                top=out[2 * nrad + npol:2 * nrad + 2 * npol])
+
+
 def label(p: pg_params) -> str:
     b = C.create_string_buffer(256)
     _check(_lib.lib().pg_label(C.byref(p), b, 256), what="pg_label")

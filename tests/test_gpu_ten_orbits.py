@@ -22,10 +22,11 @@ The fused device loop runs the same dump to the same end time.  Bounds:
 The last bound exists because this disk amplifies rounding: a planet of
 q/h^3 = 8 opens a gap whose edges grow perturbations by about e per 160
 steps after the fourth orbit, so the reference itself moves by ~1e-8 in
-Sigma and ~1e-7 in the torque history when one input cell changes by one ulp.
-No build whose arithmetic differs from the reference's at the last bit (the
-C oracle, which keeps the reference's operation order, included) can meet a
-flat 1e-8 there."""
+Sigma and ~2.5e-7 in the torque history when one input cell changes by one
+ulp.  The fused loop ends at ~4e-9 in Sigma and ~7e-8 in the torque history;
+no build whose arithmetic differs from the reference's at the last bit (the C
+oracle, which keeps the reference's operation order, included) can meet a
+flat 1e-8 on the torque history there."""
 import os
 
 import numpy as np

@@ -16,8 +16,9 @@ The fused device loop runs the same dump to the same end time.  Bounds:
 * torque history over the first 4 orbits: every step within 1e-8 of the
   largest torque;
 * final Sigma, v_phi and v_r (to the L1 of v_phi, since v_r is ~1e-3 of
-  v_phi and changes sign), and the whole torque history: relative L1 <=
-  1e-8, or 4x the reference's own 1-ulp divergence where that is larger.
+  v_phi and changes sign): relative L1 <= 1e-8;
+* the whole torque history: relative L1 <= 1e-8, or 4x the reference's own
+  1-ulp divergence where that is larger.
 
 The last bound exists because this disk amplifies rounding: a planet of
 q/h^3 = 8 opens a gap whose edges grow perturbations by about e per 160
@@ -77,6 +78,6 @@ def test_ten_orbits_match_reference_build(gpu):
           f"{e_fields[2]:.2e}, torque {e_tq:.2e}, mass {e_mass:.2e}, torque to 4 orbits {e_early:.2e}; "
           f"reference vs itself after a 1-ulp change: {sens_fields[0]:.2e}/{sens_fields[1]:.2e}/"
           f"{sens_fields[2]:.2e}, torque {sens_tq:.2e}")
-    for got, sens, name in zip(e_fields, sens_fields, ("Sigma", "v_r", "v_phi")):
-        assert got <= max(L1_TOL, SENS * sens), (name, got, sens)
+    for got, name in zip(e_fields, ("Sigma", "v_r", "v_phi")):
+        assert got <= L1_TOL, (name, got)
     assert e_tq <= max(L1_TOL, SENS * sens_tq), (e_tq, sens_tq)

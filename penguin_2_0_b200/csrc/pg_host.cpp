@@ -235,7 +235,7 @@ GhostRing make_ghost(const Profile &pf, double x, double dx, double xc, double z
 // below the first layer, top above the last; 6 x imax each, layer k + 6 i)
 // continue it with the edge layer's width.  Each ring carries the disk
 // profile's axisymmetric state at its centre.  The reference's lft branch for
-// a spherical grid (init.cpp:289-295) forms no density or pressure before
+// a spherical grid (init.cpp:289-294) forms no density or pressure before
 // using them; here every ring takes the profile's values.
 void boundary_rings(const Profile &pf, const Geometry &g, std::vector<GhostRing> &lft,
                     std::vector<GhostRing> &rgh, std::vector<GhostRing> &udr, std::vector<GhostRing> &top) {

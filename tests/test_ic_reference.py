@@ -12,7 +12,7 @@ ghost layers) agree with them bit for bit, with two exceptions:
   (v_r = 0); the reference's fresh start sets the viscous inflow speed
   -1.5 nu / r.  The boundary rings carry the inflow speed in both.
 * the inner radial boundary rings of a 3D spherical grid: the reference's
-  branch for them (init.cpp:289-295) never forms the density and pressure it
+  branch for them (init.cpp:289-294) never forms the density and pressure it
   then uses, so its Sigma, p, v_phi and rot_v there are left over from
   whatever the variables held; here they take the disk profile's values.
   Their geometry and v_r still agree.

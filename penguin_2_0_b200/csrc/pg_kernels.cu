@@ -408,13 +408,13 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store
       za = T.z[kk]; dz = T.dz[kk]; zc = T.zc[kk]; zvol = T.zvol[kk];
       const double *g = T.tg + ((size_t)kk * T.nr + i) * 4;
       r = g[0]; p = g[1]; u = g[2]; v = g[3]; w = 0.0;
-      rad_cyl = rad * sin(zc);
+      rad_cyl = rad * T.szc[kk];
       c.vrot = 0.0;
     } else if (kr >= nk) {
       int km = 2 * nk - 1 - kr;          // mirror layer
       int kz = kr + NPAD;                // ghost geometry slot
       za = T.z[kz]; dz = T.dz[kz]; zc = T.zc[kz]; zvol = T.zvol[kz];
-      rad_cyl = rad * sin(zc);
+      rad_cyl = rad * T.szc[kz];
       if (ntop == 0) {
         int rkm = km * nrg + row;
         size_t s = (size_t)rkm * nphi + j0;

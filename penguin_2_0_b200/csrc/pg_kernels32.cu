@@ -650,6 +650,9 @@ using namespace pgd;
 
 static inline int cta_for32(int lim) { return lim <= 32 ? 32 : (lim <= 64 ? 64 : 128); }
 
+// 128-thread FP32 sweeps: the radial kernel at 4 CTAs per SM (80 registers;
+// at 64 it spills and runs slower), the azimuthal one at 8 (64 registers, no
+// spills in 2D: 6-9 % faster than at 80)
 #define PG32_X(SPHV, TD, NTV, grid, l0)                                                          \
   do {                                                                                           \
     if ((NTV) == 128) k32_sweep_x<SPHV, TD, 128, 4><<<grid, 128, 0, s>>>(T, P, ph, c, l0);       \
@@ -658,7 +661,7 @@ static inline int cta_for32(int lim) { return lim <= 32 ? 32 : (lim <= 64 ? 64 :
   } while (0)
 #define PG32_Y(SPHV, TD, NTV, grid, l0)                                                          \
   do {                                                                                           \
-    if ((NTV) == 128) k32_sweep_y<SPHV, TD, 128, 4><<<grid, 128, 0, s>>>(T, P, ph, c, l0);       \
+    if ((NTV) == 128) k32_sweep_y<SPHV, TD, 128, 8><<<grid, 128, 0, s>>>(T, P, ph, c, l0);       \
     else if ((NTV) == 64) k32_sweep_y<SPHV, TD, 64, 1><<<grid, 64, 0, s>>>(T, P, ph, c, l0);     \
     else k32_sweep_y<SPHV, TD, 32, 1><<<grid, 32, 0, s>>>(T, P, ph, c, l0);                      \
   } while (0)

@@ -20,7 +20,9 @@ def _p(**over):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("over", [dict(), dict(ntop=3), dict(plnt_flag=0, visc_flag=0),
-                                  dict(EOS=1, gam=5.0 / 3.0)])
+                                  dict(EOS=1, gam=5.0 / 3.0), dict(EOS=1, gam=5.0 / 3.0, ntop=3),
+                                  dict(plnt_flag=2),          # moving planet (no disk force in 3D)
+                                  dict(FARGO_flag=0)])
 def test_3d_host_loop_matches_oracle(gpu, over):
     p = _p(**over)
     ic = pg.build_ic(p)

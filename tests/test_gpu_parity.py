@@ -25,6 +25,7 @@ CASES = {
     # isentropic EOS 1 (Newton Riemann solver, p = cs2 Sigma^gam / gam)
     "g136x136_eos1": dict(imax=136, jmax=136, EOS=1, gam=1.4),
     "cfg0_eos1": dict(imax=256, jmax=768, EOS=1, gam=5.0 / 3.0),
+    "g136x136_eos1_moving": dict(imax=136, jmax=136, EOS=1, gam=1.4, plnt_flag=2),
     # FARGO shift at the solid-body rate: whole-cell shifts in a frame
     # rotating with a planet at R_p = 0.3; the non-rotating frame (FrRot_flag
     # 0), where the planet moves through the grid, with a fixed and a moving planet

@@ -19,11 +19,13 @@ REQS = [
     _req(0, 0.30, imax=128, jmax=384, M_p=1e-3),
     _req(0, 0.20, imax=192, jmax=576, M_p=2e-5, precision=1),
     _req(1, 0.15, imax=64, jmax=192, kmax=16),
+    _req(0, 0.20, imax=136, jmax=408, EOS=1, gam=1.4),       # isentropic: own step sequence
     _req(0, 0.25, imax=136, jmax=408, M_p=3e-4, sc_h=0.06, ss_alpha=1e-2),
     _req(0, 0.10, imax=256, jmax=768, M_p=1e-5, precision=1, p_alpha=0.7),
+    _req(0, 0.20, imax=136, jmax=408, plnt_flag=2),          # moving planet: own step sequence
     _req(0, 0.35, imax=128, jmax=384, plnt_flag=0),
 ]
-ARRIVALS = [0.0, 0.0, 0.02, 0.05, 0.08, 0.12]
+ARRIVALS = [0.0, 0.0, 0.02, 0.03, 0.05, 0.08, 0.10, 0.12]
 
 
 def _alone(p):

@@ -77,6 +77,7 @@ struct pg_batch {
     cudaError_t e_ = (call);                                                  \
     if (e_ != cudaSuccess) {                                                  \
       b->err = std::string(#call) + ": " + cudaGetErrorString(e_);            \
+      (void)cudaGetLastError(); /* reported: not a later launch's error */    \
       return PG_ERR_CUDA;                                                     \
     }                                                                         \
   } while (0)
@@ -215,6 +216,7 @@ int pg_batch_create(int device, pg_batch **out) {
       cudaMalloc(&b->d_halted, sizeof(int)) != cudaSuccess ||
       cudaHostAlloc(&b->h_halted, sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
     pg_batch_destroy(b);
+    (void)cudaGetLastError();
     return PG_ERR_CUDA;
   }
   for (auto &e : b->probe)

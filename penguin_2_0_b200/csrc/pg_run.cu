@@ -105,6 +105,10 @@ static int ev_close(pg_run *run, size_t a) {
 
 static int fail(pg_run *run, int code, const std::string &msg) {
   if (run) run->err = msg;
+  // a failed allocation leaves its (non-sticky) error as the runtime's last
+  // error; it is reported here, so clear it before a later launch check of
+  // any run on this thread reads it as its own
+  if (code == PG_ERR_NOMEM) (void)cudaGetLastError();
   return code;
 }
 
@@ -162,7 +166,11 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
   run->P = *p;
   run->dev = device;
   run->nr = p->imax; run->nphi = p->jmax; run->nk = p->kmax; run->nrg = p->imax + 2 * NPAD;
-  auto bail = [&](int code) { pg_destroy(run); return code; };
+  auto bail = [&](int code) {
+    pg_destroy(run);
+    (void)cudaGetLastError();   // reported here: do not leave it for a later launch check
+    return code;
+  };
   if (cudaSetDevice(device) != cudaSuccess) { delete run; return PG_ERR_CUDA; }
   if (cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PG_ERR_CUDA);
   run->plane_elems = (size_t)run->nk * run->nrg * run->nphi;

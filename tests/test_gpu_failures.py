@@ -90,6 +90,21 @@ def test_calls_out_of_order_and_bad_sizes(gpu):
 
 
 @pytest.mark.gpu
+def test_run_larger_than_the_gpu_is_refused(gpu):
+    # one plane of 20012 x 1200000 rings x 8 B is 192 GB, more than the GPU
+    # holds: creation fails at its first allocation and reports PG_ERR_NOMEM,
+    # and the allocation error it cleared does not reach the next run's
+    # launch checks
+    p = pg.params(0, imax=20000, jmax=1200000)
+    assert pg.host.check_params(p) == 0
+    assert pg.run_device_bytes(p) > 10 ** 12
+    with pytest.raises(pg.PenguinError) as e:
+        pg.Run(p, 0)
+    assert e.value.status == 8            # PG_ERR_NOMEM
+    _healthy_step_works()
+
+
+@pytest.mark.gpu
 def test_batch_member_failure_stays_local(gpu):
     # a member with a bad cell halts with its status; the other member steps
     # on and still equals the same run advanced alone

@@ -30,7 +30,8 @@ seeded dump is loaded from pinned host memory (pg_load_rings), pg_clock_reset
 and pg_advance_graph (the ABI's replacement of main.cu's loop) run the steps,
 every step's diagnostics row (dt, mass, torque, ...) is read back (pg_history)
 and the final dump is saved to pinned host memory, all inside the timed
-region; the job runs three times and the median is reported.
+region; after one untimed job the job runs three times and the median is
+reported.
 e2e_host_loop times the reference's per-call sequence instead
 (pg_get_dt, pg_index_shift, pg_sweep2d/3d, pg_damp, pg_reduce from a Python
 loop with main.cu's host syncs: dt, planet and FrRot to the device, dt, mass
@@ -491,10 +492,12 @@ def main():
     run2.clock_reset(0)
     run2.advance(args.chunk, graph_chunk=args.chunk)     # graph capture outside the timed job
     torch.cuda.synchronize()
-    # the job runs E2E_JOBS times; the median job time is reported (one job
-    # is ~0.5 s, short enough for a one-off host or bus stall to dominate it)
+    # one untimed job first (first-use costs of the load and save staging and
+    # of the step graphs), then E2E_JOBS timed jobs; the median job time is
+    # reported (one job is ~0.5 s, short enough for a one-off host or bus
+    # stall to dominate it)
     jobs = []
-    for _ in range(E2E_JOBS):
+    for rep in range(E2E_JOBS + 1):
         _barrier(dist)
         t0 = time.perf_counter()
         run2.load_from(pin_in.data_ptr(), dump_bytes)
@@ -503,7 +506,9 @@ def main():
         hist = run2.history(max_rows=e2e_steps)
         run2.save_to(pin_out.data_ptr(), dump_bytes)
         torch.cuda.synchronize()
-        jobs.append(_max_over_ranks(dist, time.perf_counter() - t0))
+        el = _max_over_ranks(dist, time.perf_counter() - t0)
+        if rep > 0:
+            jobs.append(el)
         assert done == e2e_steps and hist.shape[0] == e2e_steps, (done, hist.shape)
     e2e_el = sorted(jobs)[len(jobs) // 2]
     e2e_value = cells * e2e_steps * ws / e2e_el
@@ -519,14 +524,16 @@ def main():
             pg.GPU_output_reduction(run3, planet, 0.0, 9)
 
     hl_jobs = []
-    for _ in range(E2E_JOBS):
+    for rep in range(E2E_JOBS + 1):
         _barrier(dist)
         t0 = time.perf_counter()
         run3.load_from(pin_in.data_ptr(), dump_bytes)
         run3.kernel_loop(e2e_steps, record=rec)
         run3.save_to(pin_out.data_ptr(), dump_bytes)
         torch.cuda.synchronize()
-        hl_jobs.append(_max_over_ranks(dist, time.perf_counter() - t0))
+        el = _max_over_ranks(dist, time.perf_counter() - t0)
+        if rep > 0:
+            hl_jobs.append(el)
     hl_el = sorted(hl_jobs)[len(hl_jobs) // 2]
     hl_value = cells * e2e_steps * ws / hl_el
     run3.close()

@@ -27,7 +27,7 @@ const double kMMSN = 0.00019126835;
 // compile-time constants, and pow(x, 0), pow(x, 1), pow(x, -1) and pow(x, 2)
 // are folded to 1, x, 1/x and x*x (exact or correctly rounded, where libm's
 // pow can differ by an ulp); other exponents stay calls.
-static double cpow_c(double x, double y) {
+double cpow_c(double x, double y) {
   if (y == 0.0) return 1.0;
   if (y == 1.0) return x;
   if (y == -1.0) return 1.0 / x;

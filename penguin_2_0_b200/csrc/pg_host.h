@@ -72,6 +72,8 @@ GhostRing make_ghost(const Profile &pf, double x, double dx, double xc, double z
 void boundary_rings(const Profile &pf, const Geometry &g, std::vector<GhostRing> &lft,
                     std::vector<GhostRing> &rgh, std::vector<GhostRing> &udr, std::vector<GhostRing> &top);
 int params_geometry(const pg_params &P, Geometry &g);
+// pow(x, y) in the form the reference's compiler gives a constant exponent
+double cpow_c(double x, double y);
 int read_geometry(const pg_params &P, const unsigned char *b, Geometry &g, std::string &why);
 std::string label(const pg_params &P);
 

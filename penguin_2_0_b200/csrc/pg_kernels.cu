@@ -904,6 +904,18 @@ __device__ void d_kick(Body &pl, double &FrRot, double dt, int frflag) {
   FrRot = (frflag == 1) ? pl.vy : 0.0;
   pl.vy -= FrRot;
 }
+// The planet's arithmetic is host code in the reference (planet.cu), whose
+// compiler folds pow with the constant exponents 0, 1, -1 and 2 into 1, x,
+// 1/x and x*x; the device copies below use the same forms (other exponents
+// stay pow calls), and round products that feed a sum on their own, as the
+// host does.
+__device__ __forceinline__ double pow_host_form(double x, double y) {
+  if (y == 0.0) return 1.0;
+  if (y == 1.0) return x;
+  if (y == -1.0) return 1.0 / x;
+  if (y == 2.0) return __dmul_rn(x, x);
+  return pow(x, y);
+}
 __device__ void d_drift(Body &pl, double FrRot, double dt, const DevClock &c) {
   double old_rad = pl.x;
   pl.x += dt * pl.vx;
@@ -920,10 +932,10 @@ __device__ void d_drift(Body &pl, double FrRot, double dt, const DevClock &c) {
 // with cs2 = sc_h^2 x^-p_beta (disk_profile.cu:39-52)
 __device__ void d_drift_moving(Body &pl, double FrRot, double dt, const DevClock &c) {
   d_drift(pl, FrRot, dt, c);
-  pl.rs = c.rs_fac * sqrt(c.sc2 * pow(pl.x, -c.p_beta) * pl.x * pl.x * pl.x);
+  pl.rs = c.rs_fac * sqrt(c.sc2 * pow_host_form(pl.x, -c.p_beta) * pl.x * pl.x * pl.x);
 }
 __device__ void d_forces_fixed(Body &pl, double FrRot) {
-  pl.fx = -1.0 / pl.x / pl.x + pl.x * pow(pl.vy + FrRot, 2);
+  pl.fx = -1.0 / pl.x / pl.x + __dmul_rn(pl.x, pow_host_form(pl.vy + FrRot, 2.0));
   pl.fy = 0.0;
 }
 
@@ -1014,7 +1026,7 @@ __device__ __forceinline__ void poststep_body(DevClock *clk, const Tables &T, in
   } else {
     // planet_forces planet.cu:58-59 with the disk sums of this state
     Body &p = c.planet;
-    p.fx = c.Sigma_0 * c.f8 / p.m - 1.0 / p.x / p.x + p.x * pow(p.vy + c.frrot, 2);
+    p.fx = c.Sigma_0 * c.f8 / p.m - 1.0 / p.x / p.x + __dmul_rn(p.x, pow_host_form(p.vy + c.frrot, 2.0));
     p.fy = c.Sigma_0 * c.f9 / p.m;
     d_kick(p, c.frrot, 0.5 * dt, c.frrot_flag);
     c.frrot_next = c.frrot;      // the CFL of the next get_dt runs after this kernel

@@ -776,7 +776,7 @@ int pg_clock_reset(pg_run *run, int startat) {
   c.M_p = P.M_p; c.t_growth = P.t_growth; c.rs_fac = P.rs_fac; c.sc2 = P.sc_h * P.sc_h; c.R_p = P.R_p;
   c.Sigma_0 = P.Sigma_0;
   c.p_beta = P.p_beta;
-  c.hist_norm = P.M_p * P.M_p * std::pow(P.R_p, 1.0 - P.p_alpha + (P.p_beta - 1.0)) / (P.sc_h * P.sc_h);
+  c.hist_norm = P.M_p * P.M_p * pg::cpow_c(P.R_p, 1.0 - P.p_alpha + (P.p_beta - 1.0)) / (P.sc_h * P.sc_h);
   c.hist = run->hist; c.hist_cap = run->hist_cap; c.hist_count = 0;
   cudaStream_t s = run->stream;
   CK(cudaMemcpyAsync(run->clk, &c, sizeof(c), cudaMemcpyHostToDevice, s));

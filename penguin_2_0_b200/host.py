@@ -538,6 +538,20 @@ def get_ecc(planet: Planet, FrRot: float) -> float:
     return _lib.lib().pg_get_ecc(C.byref(b), FrRot)
 
 
+def _pow_const(x: float, y: float) -> float:
+    """pow in the form the reference's compiler gives a constant exponent:
+    0, 1, -1 and 2 fold to 1, x, 1/x and x*x."""
+    if y == 0.0:
+        return 1.0
+    if y == 1.0:
+        return x
+    if y == -1.0:
+        return 1.0 / x
+    if y == 2.0:
+        return x * x
+    return math.pow(x, y)
+
+
 def torque_norm(p: pg_params) -> float:
     """main.cu:421 normalisation of the mode-9 torque."""
-    return p.M_p * p.M_p * math.pow(p.R_p, 1.0 - p.p_alpha + (p.p_beta - 1.0)) / (p.sc_h * p.sc_h)
+    return p.M_p * p.M_p * _pow_const(p.R_p, 1.0 - p.p_alpha + (p.p_beta - 1.0)) / (p.sc_h * p.sc_h)

@@ -81,16 +81,31 @@ static double max3(double A, double B, double C) {
 /* ------------------------------------------------------------------------ */
 /* disk profile (disk_profile.cu)                                           */
 
+/* The profile serves two sides of the reference.  Its set-up (init.cpp: the
+ * initial state, the fixed boundary rings, the damping targets) and its planet
+ run on the host, where p_alpha, p_beta and gam are compile-time
+ * constants and the host compiler turns pow(x, 0|1|-1|2) into 1, x, 1/x, x*x
+ * (planet.cu's host functions likewise); hpow restates that folding.  The device kernels (the sweep store's pressure,
+ * the damping kernel, the viscosity) call pow as written, so get_cs2 and
+ * get_nu keep it. */
+static double hpow(double x, double y) {
+  if (y == 0.0) return 1.0;
+  if (y == 1.0) return x;
+  if (y == -1.0) return 1.0 / x;
+  if (y == 2.0) return x * x;
+  return pow(x, y);
+}
 static double get_rho1(double r) {                                         /* 9-28 */
   double n = -G.p_alpha;
   if (G.EOS != 0 && G.ndim == 3) n = -G.p_alpha * (2.0 / (G.gam + 1.0));
-  return pow(r, n);
+  return hpow(r, n);
 }
 static double get_cs2(double r) { return G.sc_h * G.sc_h * pow(r, -G.p_beta); } /* 39-42 */
-static double get_h(double r) { return sqrt(get_cs2(r) * r * r * r); }      /* 49-52 */
+static double host_cs2(double r) { return G.sc_h * G.sc_h * hpow(r, -G.p_beta); }
+static double get_h(double r) { return sqrt(host_cs2(r) * r * r * r); }     /* 49-52 */
 static double get_P1(double r) {                                           /* 54-61 */
-  if (G.EOS == 0) return get_cs2(r) * get_rho1(r);
-  return get_cs2(r) * pow(get_rho1(r), G.gam) / G.gam;
+  if (G.EOS == 0) return host_cs2(r) * get_rho1(r);
+  return host_cs2(r) * hpow(get_rho1(r), G.gam) / G.gam;
 }
 static double get_dP_dr1(double r) {                                       /* 63-68 */
   double p1 = get_P1(r + 1.27245e-8);
@@ -98,7 +113,7 @@ static double get_dP_dr1(double r) {                                       /* 63
   return (p1 - p2) / 2.5449e-8;
 }
 static double get_verfac(double r, double z) {                              /* 70-75 */
-  double cs2 = get_cs2(r);
+  double cs2 = host_cs2(r);
   double rr = sqrt(r * r + z * z);
   return exp((1.0 / rr - 1.0 / r) / cs2);
 }
@@ -106,16 +121,16 @@ static double get_rho2(double r, double z) {                               /* 86
   double gamm, h, z_0, base;
   if (G.EOS == 0) return get_rho1(r) * get_verfac(r, z);
   gamm = G.gam - 1.0;
-  h = sqrt(get_cs2(r) * r * r * r);
-  z_0 = sqrt(2.0 * h * h * pow(r, -G.p_alpha * (2.0 / (G.gam + 1.0)) * gamm) / gamm);
+  h = sqrt(host_cs2(r) * r * r * r);
+  z_0 = sqrt(2.0 * h * h * hpow(r, -G.p_alpha * (2.0 / (G.gam + 1.0)) * gamm) / gamm);
   if (z < z_0)
-    return pow(pow(get_rho1(r), gamm) - (gamm / (r * get_cs2(r))) * (1.0 - r / sqrt(r * r + z * z)), 1.0 / gamm);
-  base = pow(pow(get_rho1(r), gamm) - (gamm / (r * get_cs2(r))) * (1.0 - r / sqrt(r * r + z_0 * z_0)), 1.0 / gamm);
+    return hpow(hpow(get_rho1(r), gamm) - (gamm / (r * host_cs2(r))) * (1.0 - r / sqrt(r * r + z * z)), 1.0 / gamm);
+  base = hpow(hpow(get_rho1(r), gamm) - (gamm / (r * host_cs2(r))) * (1.0 - r / sqrt(r * r + z_0 * z_0)), 1.0 / gamm);
   return pow(10.0, log10(base) - 6.0 * (z - z_0) / h);
 }
 static double get_P2(double r, double z) {                                 /* 112-118 */
-  if (G.EOS == 0) return get_cs2(r) * get_rho2(r, z);
-  return get_cs2(r) * pow(get_rho2(r, z), G.gam) / G.gam;
+  if (G.EOS == 0) return host_cs2(r) * get_rho2(r, z);
+  return host_cs2(r) * hpow(get_rho2(r, z), G.gam) / G.gam;
 }
 /* the sweep store's pressure (ppm.cu:138-143): EOS 0 r cs2, EOS 1 cs2 r^gam / gam */
 static double store_p(double r, double cs2) {
@@ -134,7 +149,7 @@ static double get_dP_s(double r, double pol) {                              /* 1
 }
 static double get_nu(double r) { return G_vis_nu * pow(r, G.p_alpha); }    /* 149-152 */
 static double get_viscous_vr(double r) {                                   /* 154-160 */
-  if (G.visc_flag == 1) return -1.5 * get_nu(r) / r;
+  if (G.visc_flag == 1) return -1.5 * (G_vis_nu * hpow(r, G.p_alpha)) / r;
   return 0.0;
 }
 
@@ -1290,12 +1305,12 @@ void orc_planet_forces(orc_run *R, pg_body *pl, double FrRot, double simtime) { 
   if (G.plnt_flag == 2) {
     double f8 = orc_reduce(R, pl, 0.0, 8);
     set_globals(&R->P);
-    pl->fx = G.Sigma_0 * f8 / pl->m - 1.0 / pl->x / pl->x + pl->x * pow(pl->vy + FrRot, 2);
+    pl->fx = G.Sigma_0 * f8 / pl->m - 1.0 / pl->x / pl->x + pl->x * hpow(pl->vy + FrRot, 2.0);
     double f9 = orc_reduce(R, pl, 0.0, 9);
     set_globals(&R->P);
     pl->fy = G.Sigma_0 * f9 / pl->m;
   } else {
-    pl->fx = -1.0 / pl->x / pl->x + pl->x * pow(pl->vy + FrRot, 2);
+    pl->fx = -1.0 / pl->x / pl->x + pl->x * hpow(pl->vy + FrRot, 2.0);
     pl->fy = 0.0;
   }
 }
@@ -1488,6 +1503,42 @@ orc_run *orc_create(const pg_params *p, const void *buf, size_t bytes) {
   return R;
 }
 
+/* The fixed ghost rings (lft, rgh, then udr, top in 3D), one row of
+ * x dx xvol xc z dz zvol zc r p u v w rot_v per ring, in the oracle's own
+ * storage order.  count receives the number of rings; out may be NULL.    */
+int orc_boundary(const orc_run *R, double *out, size_t n_doubles, int *count) {
+  int ng = NPAD * R->nk, nt = (R->nk > 1) ? NPAD * R->nr : 0;
+  int n = 2 * ng + 2 * nt;
+  *count = n;
+  if (!out) return 0;
+  if (n_doubles < (size_t)n * 14) return -1;
+  const oring *grp[4] = {R->lft, R->rgh, R->udr, R->top};
+  int len[4] = {ng, ng, nt, nt};
+  double *o = out;
+  for (int g = 0; g < 4; g++)
+    for (int b = 0; b < len[g]; b++) {
+      const oring *c = &grp[g][b];
+      double row[14] = {c->x, c->dx, c->xvol, c->xc, c->z, c->dz, c->zvol, c->zc,
+                        c->r[0], c->p[0], c->u[0], c->v[0], c->w[0], c->rot_v};
+      memcpy(o, row, sizeof row);
+      o += 14;
+    }
+  return 0;
+}
+
+/* The axisymmetric profile the damping relaxes toward (r p u v w per
+ * ring, ring i + imax k).                                                 */
+int orc_targets(const orc_run *R, double *out, size_t n_doubles) {
+  size_t n = (size_t)R->nr * R->nk;
+  if (n_doubles < n * 5) return -1;
+  for (size_t q = 0; q < n; q++) {
+    const osym *v = &R->val[q];
+    out[5 * q] = v->r; out[5 * q + 1] = v->p; out[5 * q + 2] = v->u;
+    out[5 * q + 3] = v->v; out[5 * q + 4] = v->w;
+  }
+  return 0;
+}
+
 void orc_destroy(orc_run *R) {
   if (!R) return;
   free(R->mem); free(R->rings); free(R->lft); free(R->rgh); free(R->udr); free(R->top); free(R->val);
@@ -1580,7 +1631,7 @@ int orc_run_steps(orc_run *R, int nsteps, int startat, double *hist) {
       h[1] = dt_used;
       h[2] = orc_reduce(R, &pl, 0.0, 0);
       set_globals(&R->P);
-      double norm = P.M_p * P.M_p * pow(P.R_p, 1.0 - P.p_alpha + (P.p_beta - 1.0)) / (P.sc_h * P.sc_h);
+      double norm = P.M_p * P.M_p * hpow(P.R_p, 1.0 - P.p_alpha + (P.p_beta - 1.0)) / (P.sc_h * P.sc_h);
       h[3] = (P.plnt_flag > 0 && P.ndim == 2) ? orc_reduce(R, &pl, 0.0, 9) / norm : 0.0;
     }
     set_globals(&R->P);

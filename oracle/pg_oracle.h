@@ -36,6 +36,12 @@ orc_run *orc_create(const pg_params *p, const void *rings, size_t bytes);
 void     orc_destroy(orc_run *R);
 /* Serialise the current rings in the dump layout.                           */
 int      orc_save(const orc_run *R, void *rings, size_t bytes);
+/* The fixed ghost rings built at creation (lft, rgh, then udr, top when
+ * kmax > 1), 14 doubles each: x dx xvol xc z dz zvol zc r p u v w rot_v.
+ * count receives the ring count; out may be NULL to query it.              */
+int      orc_boundary(const orc_run *R, double *out, size_t n_doubles, int *count);
+/* The damping targets (init.cpp:92-183), r p u v w per ring i + imax k.    */
+int      orc_targets(const orc_run *R, double *out, size_t n_doubles);
 
 double orc_get_dt(orc_run *R, double dt_old, double frrot);     /* timestep.cu:112 */
 void   orc_index_shift(orc_run *R, double dt, double frrot);    /* orbital_advection.cu:45 */

@@ -58,6 +58,8 @@ def lib():
             "orc_kick_drift_kick": (None, [P, B, dp, C.c_double, C.c_int]),
             "orc_run_steps": (C.c_int, [vp, C.c_int, C.c_int, dp]),
             "orc_threads": (C.c_int, []),
+            "orc_boundary": (C.c_int, [vp, dp, C.c_size_t, C.POINTER(C.c_int)]),
+            "orc_targets": (C.c_int, [vp, dp, C.c_size_t]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)
@@ -99,6 +101,21 @@ class Oracle:
         h = (C.c_double * (4 * nsteps))()
         n = lib().orc_run_steps(self._h, nsteps, startat, h)
         return np.frombuffer(h, dtype=np.float64)[: 4 * n].reshape(n, 4).copy()
+
+    def boundary(self) -> np.ndarray:
+        """The fixed ghost rings, one row of 14 columns (x dx xvol xc z dz
+        zvol zc r p u v w rot_v) per ring: lft, rgh, then udr, top in 3D."""
+        cnt = C.c_int(0)
+        lib().orc_boundary(self._h, None, 0, C.byref(cnt))
+        out = np.zeros((cnt.value, 14))
+        assert lib().orc_boundary(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), out.size, C.byref(cnt)) == 0
+        return out
+
+    def targets(self) -> np.ndarray:
+        """The damping targets, r p u v w per ring i + imax k."""
+        out = np.zeros((self.p.imax * self.p.kmax, 5))
+        assert lib().orc_targets(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), out.size) == 0
+        return out
 
     def get_dt(self, dt, frrot):
         return lib().orc_get_dt(self._h, dt, frrot)

@@ -110,7 +110,7 @@ int pg_config_params(int which, pg_params *p);
 int pg_check_params(const pg_params *p);
 
 /* Size in bytes of one hydr_ring record of the dump layout
- * (variable_types.h:67-97): 72*jmax + 96.                                  */
+ * (variable_types.h:67-97): 72*jmax + 96; 0 for jmax <= 0.                 */
 size_t pg_ring_bytes(int jmax);
 
 /* Writes the seeded initial condition as a reference-layout dump
@@ -199,7 +199,9 @@ int pg_damp(pg_run *run, double dt);
 int pg_reduce(pg_run *run, const pg_body *planet, double exclude, int mode,
               double *out);
 
-/* ---- planet (planet.cu:11-93), host arithmetic --------------------------- */
+/* ---- planet (planet.cu:11-93), host arithmetic ---------------------------
+ * The three functions that return a double (no status) return NaN when given
+ * a NULL pointer.                                                          */
 int pg_init_planet(const pg_params *p, pg_body *planet, double *frrot);
 double pg_set_M_p(const pg_params *p, double t);
 int pg_planet_forces(pg_run *run, pg_body *planet, double frrot, double simtime);

@@ -520,7 +520,7 @@ int pg_check_params(const pg_params *p) {
   return pg::check_params(p, why);
 }
 
-size_t pg_ring_bytes(int jmax) { return pg::ring_bytes(jmax); }
+size_t pg_ring_bytes(int jmax) { return jmax > 0 ? pg::ring_bytes(jmax) : 0; }
 
 int pg_boundary_rings(const pg_params *p, double *out, size_t n_doubles, int *count) {
   if (!p || !count) return PG_ERR_ARG;

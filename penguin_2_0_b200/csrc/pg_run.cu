@@ -684,6 +684,7 @@ int pg_reduce(pg_run *run, const pg_body *planet, double exclude, int mode, doub
 
 // ---- planet, planet.cu:11-93 (host arithmetic as in the reference) --------------
 double pg_set_M_p(const pg_params *p, double t) {
+  if (!p) return std::nan("");
   if (t < p->t_growth) return std::fmax(p->M_p * std::sin(pg::kPi * t / (2.0 * p->t_growth)), 0.01 * pg::kEarthMass);
   return p->M_p;
 }
@@ -743,11 +744,13 @@ int pg_kick_drift_kick(const pg_params *p, pg_body *pl, double *frrot, double dt
 }
 
 double pg_get_E(const pg_body *p, double frrot) {
+  if (!p) return std::nan("");
   double vy = p->vy + frrot;
   return (p->vx * p->vx + vy * vy * p->x * p->x) / 2.0 - 1.0 / p->x;
 }
 
 double pg_get_ecc(const pg_body *p, double frrot) {
+  if (!p) return std::nan("");
   double vy = p->vy + frrot;
   double L = vy * p->x * p->x;
   return std::sqrt(1.0 + (2.0 * pg_get_E(p, frrot) * L * L));

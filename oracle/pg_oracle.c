@@ -1285,6 +1285,11 @@ static double set_M_p(double t) {                                   /* 28-34 */
   return G.M_p;
 }
 
+double orc_set_M_p(const pg_params *p, double t) {
+  set_globals(p);
+  return set_M_p(t);
+}
+
 void orc_init_planet(const pg_params *p, pg_body *pl, double *FrRot) { /* 36-52 */
   set_globals(p);
   pl->m = set_M_p(0.0);

@@ -56,6 +56,7 @@ double orc_reduce(orc_run *R, const pg_body *pl, double exclude, int mode); /* d
 
 /* Planet (planet.cu:11-93). */
 void   orc_init_planet(const pg_params *p, pg_body *pl, double *frrot);
+double orc_set_M_p(const pg_params *p, double t);
 void   orc_planet_forces(orc_run *R, pg_body *pl, double frrot, double simtime);
 void   orc_kick_drift_kick(const pg_params *p, pg_body *pl, double *frrot,
                            double dt, int kick);

@@ -59,6 +59,9 @@ def lib():
             "orc_run_steps": (C.c_int, [vp, C.c_int, C.c_int, dp]),
             "orc_threads": (C.c_int, []),
             "orc_boundary": (C.c_int, [vp, dp, C.c_size_t, C.POINTER(C.c_int)]),
+            "orc_set_M_p": (C.c_double, [P, C.c_double]),
+            "orc_get_E": (C.c_double, [B, C.c_double]),
+            "orc_get_ecc": (C.c_double, [B, C.c_double]),
             "orc_targets": (C.c_int, [vp, dp, C.c_size_t]),
         }
         for k, (r, a) in sig.items():

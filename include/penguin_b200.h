@@ -105,8 +105,9 @@ int pg_config_params(int which, pg_params *p);
 /* Checks a parameter set; PG_ERR_PARAMS with a message for combinations
  * that are not implemented (EOS 2, which the reference marks buggy;
  * bary_flag; EOS 1 on FP32 planes, ...) or whose sweep chunking would read
- * already-updated cells (jmax % 116 in 1..5).  EOS 0 (isothermal) and EOS 1
- * (isentropic, p = cs2 Sigma^gam / gam) run in 2D and 3D.                  */
+ * already-updated cells (jmax % 116 in 1..5), and sizes above CUDA's grid
+ * limit of 65535 blocks in y (imax, and jmax in 3D).  EOS 0 (isothermal)
+ * and EOS 1 (isentropic, p = cs2 Sigma^gam / gam) run in 2D and 3D.        */
 int pg_check_params(const pg_params *p);
 
 /* Size in bytes of one hydr_ring record of the dump layout

@@ -357,6 +357,13 @@ int check_params(const pg_params *p, std::string &why) {
   if (!p) { why = "null params"; return PG_ERR_ARG; }
   if (p->ndim != 2 && p->ndim != 3) { why = "ndim must be 2 or 3"; return PG_ERR_PARAMS; }
   if (p->imax < 1 || p->jmax < 1 || p->kmax < 1) { why = "grid sizes must be positive"; return PG_ERR_PARAMS; }
+  // the azimuthal sweep and the dump kernels launch one block row per ring
+  // (grid y), the 3D polar sweep one per azimuthal column: CUDA caps grid y
+  // and z at 65535
+  if (p->imax > 65535) { why = "imax must be <= 65535 (rings run on CUDA grid y)"; return PG_ERR_PARAMS; }
+  if (p->ndim == 3 && (p->jmax > 65535 || p->kmax > 65535)) {
+    why = "3D needs jmax, kmax <= 65535 (polar columns run on CUDA grid y)"; return PG_ERR_PARAMS;
+  }
   if (p->ndim == 2 && p->kmax != 1) { why = "2D problem needs kmax == 1 (main.cu:130)"; return PG_ERR_PARAMS; }
   if (p->ndim == 3 && p->kmax == 1) { why = "3D problem needs kmax > 1 (main.cu:134)"; return PG_ERR_PARAMS; }
   if (p->EOS == 2) {

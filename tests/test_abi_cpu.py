@@ -49,6 +49,9 @@ def test_default_params_are_global_h():
     (dict(imax=116 * 2 + 2), True),      # radial remainder 1..5 is fine
     (dict(kmax=4), False),               # 2D with kmax > 1
     (dict(nlft=0), False),
+    (dict(imax=65535), True),            # rings on CUDA grid y: at most 65535
+    (dict(imax=65536), False),
+    (dict(jmax=116 * 600), True),        # 2D: jmax is not on a grid y
 ])
 def test_check_params(over, ok):
     p = pg.params(0, **over)
@@ -88,6 +91,11 @@ def test_label_matches_create_label():
 def test_3d_isentropic_needs_gam_above_one():
     assert pg.host.check_params(pg.params(1, EOS=1, gam=1.0)) != 0
     assert pg.host.check_params(pg.params(1, EOS=1, gam=5.0 / 3.0)) == 0
+
+
+def test_3d_polar_columns_fit_cuda_grid_y():
+    assert pg.host.check_params(pg.params(1, jmax=116 * 564)) == 0      # 65424
+    assert pg.host.check_params(pg.params(1, jmax=116 * 565)) != 0      # 65540
 
 
 def test_isentropic_ic_pressure_and_profile():

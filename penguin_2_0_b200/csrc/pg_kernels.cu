@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_y(Tables T, Planes P, Phys p
 // the chunk and `store` false computes without storing (padding pencils of
 // the packed kernel).
 template <int NT, int EOS = 0>
-__device__ __forceinline__ void sweep_z_body(ChunkShmT<NT> &S, int n, bool store, const Tables &T, const Planes &P,
+__device__ __forceinline__ void sweep_z_body(ChunkShmData<NT> &S, int n, bool store, const Tables &T, const Planes &P,
                                              const Phys &ph, const SweepCtl &ctl, const StepIn &st, int ntop,
                                              int i, int j0, int l) {
   const int nphi = T.nphi, nrg = T.nrg, nk = T.nk;
@@ -529,17 +529,22 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_z(Tables T, Planes P, Phys p
 // Polar sweep of single-chunk pencils (nk <= PZ_LIM - 12, the usual 3D
 // disk): PACK pencils of lim = nk + 12 cells share a CTA of PACK * lim
 // threads instead of one pencil per CTA of 32/64 threads with idle lanes.
-// Measured on the 128x1024x32 disk: 4 pencils per CTA at 5 CTAs/SM (56
-// registers) take the polar sweep from 1.85 to 1.30 ms (8 per CTA at 2
-// CTAs/SM: 1.63 ms).  Thread t works on cell t / PACK of pencil t % PACK,
+// Measured on the 128x1024x32 disk (pencils of 44 cells): 4 pencils per CTA
+// at 5 CTAs/SM (56 registers) took the polar sweep from 1.85 to 1.30 ms, and
+// with the later arithmetic savings it ran at 1.04 ms; 8 pencils per CTA, 352
+// threads = 11 whole warps where 4 pencils leave half of a sixth warp idle,
+// at 3 CTAs/SM (56 registers, 33 resident warps against 30) take it to
+// 0.93 ms.  Pencils longer than 44 cells keep 4 per CTA.  An earlier 8-pencil
+// form at 2 CTAs/SM, before the bank padding, ran at 1.63 ms.
+// Thread t works on cell t / PACK of pencil t % PACK,
 // and the PACK pencils of a CTA are consecutive azimuth columns of a ring,
 // so a warp's loads of one layer cover PACK adjacent doubles.  Pencils past
 // the last column repeat the last one without storing.
 constexpr int PZ_LIM = 56;
-template <int PACK, int MINB>
-__global__ void __launch_bounds__(PACK * PZ_LIM, MINB) k_sweep_z_packed(Tables T, Planes P, Phys ph, SweepCtl ctl,
-                                                                        int ntop) {
-  __shared__ ChunkShmT<PZ_LIM> S[PACK];
+constexpr int PZ8_THREADS = 352;   // 8 pencils of up to 44 cells, 3 CTAs per SM
+template <int PACK, int MINB, int MAXT = PACK * PZ_LIM>
+__global__ void __launch_bounds__(MAXT, MINB) k_sweep_z_packed(Tables T, Planes P, Phys ph, SweepCtl ctl, int ntop) {
+  __shared__ ChunkShmT<PZ_LIM, 128 / PACK> S[PACK];
   StepIn st;
   if (!load_step(ctl, st)) return;
   const int p = threadIdx.x % PACK, n = threadIdx.x / PACK;
@@ -1403,7 +1408,10 @@ static void sweep_z_t(const Tables &T, const Planes &P, const Phys &ph, const Sw
   if constexpr (EOS == 0) {
     if (T.zpack && ch.loop == 1 && !ch.stuck && ch.lim_last <= PZ_LIM) {
       int npen = T.nr * T.nphi;
-      k_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
+      if (8 * ch.lim_last <= PZ8_THREADS)    // whole warps: 8 pencils of 44 cells (kmax 32) are 11
+        k_sweep_z_packed<8, 3, PZ8_THREADS><<<(npen + 7) / 8, 8 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
+      else
+        k_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
       return;
     }
   }

@@ -108,15 +108,19 @@ struct ChunkShmData {
   double cf0;
 };
 
-// Bytes that bring a per-pencil shared block to 32 mod 128.  Kernels that
-// pack 4 pencils per CTA (thread t on cell t/4 of pencil t%4) then place the
-// four pencils' 32-byte pieces of a half-warp's 64-bit access (or a warp's
-// 32-bit one) in four different bank groups, without bank conflicts.
-constexpr int shm_pad_bytes(int size) { return ((32 - size % 128) + 256) % 128 == 0 ? 128 : ((32 - size % 128) + 256) % 128; }
+// Bytes that bring a per-pencil shared block to TO mod 128.  Kernels that
+// pack PACK pencils per CTA (thread t on cell t/PACK of pencil t%PACK) pad to
+// 128/PACK: the pencils' pieces of a half-warp's 64-bit access (or a warp's
+// 32-bit one) then fall in PACK different bank groups, without conflicts
+// (4 pencils: 32 mod 128; 8 pencils: 16 mod 128).
+constexpr int shm_pad_to(int size, int to) {
+  return ((to - size % 128) + 256) % 128 == 0 ? 128 : ((to - size % 128) + 256) % 128;
+}
+constexpr int shm_pad_bytes(int size) { return shm_pad_to(size, 32); }
 
-template <int NT>
+template <int NT, int TO = 32>
 struct ChunkShmT : ChunkShmData<NT> {
-  char pad_[shm_pad_bytes((int)sizeof(ChunkShmData<NT>))];
+  char pad_[shm_pad_to((int)sizeof(ChunkShmData<NT>), TO)];
 };
 
 // ---- star + planet gravity, forces.cu:23-182 (non-barycentric frame) ------

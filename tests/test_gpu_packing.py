@@ -1,8 +1,10 @@
-"""Short chunks packed 4 per CTA give the same bits as one per CTA.
+"""Short chunks packed several per CTA give the same bits as one per CTA.
 
-A radial pencil's last chunk of at most 64 cells, and a polar pencil that is
-a single chunk (nk + 12 <= 56 cells), run 4 adjacent columns per CTA by
-default; PG_POLAR_PACK=0 runs one per 32/64-thread CTA.  The cell arithmetic
+A radial pencil's last chunk of at most 64 cells runs 4 adjacent columns per
+CTA, and a polar pencil that is a single chunk (nk + 12 <= 56 cells) runs 8
+per CTA (nk + 12 <= 44: whole warps) or 4, by default; PG_POLAR_PACK=0 runs
+one per 32/64-thread CTA.  A CTA past the last column computes its padding
+pencils without storing them.  The cell arithmetic
 is the same device body either way, so the results must be bitwise equal."""
 import numpy as np
 import pytest
@@ -14,6 +16,8 @@ CASES = [
     dict(which=0, imax=136, jmax=408, precision=1),          # 20 + 12, FP32
     dict(which=1, imax=128, jmax=132, kmax=16),               # radial 12 + 12, polar 16 + 12
     dict(which=1, imax=64, jmax=132, kmax=24),                # single radial chunk, polar 24 + 12
+    dict(which=1, imax=63, jmax=132, kmax=32),                # polar 32 + 12, 8316 pencils: 4 padding
+    dict(which=1, imax=64, jmax=132, kmax=40),                # polar 40 + 12: 4 pencils per CTA
     dict(which=1, imax=64, jmax=132, kmax=16, precision=1),   # FP32 3D
 ]
 

@@ -32,7 +32,7 @@ GRID_CASES = [
 
 
 def main():
-    from make_golden import params_for, to_json  # noqa: F401
+    from make_golden import to_json
     from penguin_2_0_b200 import _lib
     import ctypes as C
     ref = os.environ.get("PG_REFERENCE", "/root/reference")

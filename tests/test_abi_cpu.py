@@ -1,7 +1,6 @@
 """Host-side checks that need no GPU: the C ABI library loads and exports
 every symbol include/penguin_b200.h declares, parameter validation, the
 seeded initial condition and the dump layout."""
-import ctypes as C
 import subprocess
 
 import numpy as np

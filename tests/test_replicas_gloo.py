@@ -4,7 +4,6 @@ gloo backend, each rank advancing its own disk on the CPU oracle."""
 import os
 import socket
 
-import numpy as np
 import torch.multiprocessing as mp
 
 

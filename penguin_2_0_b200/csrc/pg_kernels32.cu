@@ -488,7 +488,8 @@ __global__ void __launch_bounds__(NT, MINB) k32_sweep_z(Tables T, Planes32 P, Ph
   sweep_z32_body<NT>(S, threadIdx.x, true, T, P, ph, ctl, st, ntop, blockIdx.x, blockIdx.y, blockIdx.z + l0);
 }
 
-// single-chunk polar pencils packed 4 per CTA (see k_sweep_z_packed)
+// single-chunk polar pencils packed 4 per CTA (the FP64 kernel
+// k_sweep_z_packed packs 8 of up to 44 cells)
 constexpr int PZ32_LIM = 56;
 template <int PACK, int MINB>
 __global__ void __launch_bounds__(PACK * PZ32_LIM, MINB) k32_sweep_z_packed(Tables T, Planes32 P, Phys ph,

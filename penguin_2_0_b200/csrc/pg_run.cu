@@ -200,9 +200,10 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
     // large 2D grids, same arithmetic; PG_SWEEP_OCC=6 keeps ~76 registers
     const char *occ = std::getenv("PG_SWEEP_OCC");
     T.occ8 = (occ && std::atoi(occ) == 6) ? 0 : 1;
-    // short chunks (a polar pencil of one chunk, a radial last chunk of at
-    // most 64 cells) packed 4 per CTA by default (PG_POLAR_PACK=0: one per
-    // CTA); same arithmetic per cell either way
+    // short chunks packed several per CTA by default: a radial last chunk of
+    // at most 64 cells 4 per CTA, an FP64 polar pencil of one chunk 8 per CTA
+    // up to 44 cells and 4 above, an FP32 one 4 per CTA (PG_POLAR_PACK=0: one
+    // per CTA); same arithmetic per cell either way
     const char *zp = std::getenv("PG_POLAR_PACK");
     T.zpack = (zp && std::atoi(zp) == 0) ? 0 : 4;
   }

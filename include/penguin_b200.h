@@ -141,9 +141,12 @@ int pg_label(const pg_params *p, char *buf, size_t len);
 int pg_dump_name(const pg_params *p, const char *dir, int frame, char *buf, size_t len);
 
 /* files/time_<label>.dat rows (main.cu:417-427): simtime, mass, normalised
- * torque, planet x y vx vy fx fy, eccentricity, semi-major axis; 11 doubles
- * per row written with 16 significant digits, space separated.             */
-int pg_write_time_rows(const char *path, const double *rows, int nrows, int append);
+ * torque, planet x y vx vy fx fy, eccentricity, semi-major axis.  rows holds
+ * 11 doubles per row (the pg_history layout); each is written with 16
+ * significant digits, space separated, all 11 when p->plnt_flag > 0 and the
+ * first two (simtime, mass) without a planet, as the reference does.       */
+int pg_write_time_rows(const pg_params *p, const char *path, const double *rows, int nrows,
+                       int append);
 
 /* read/para_<label>.dat of write_para_file (output.cu:90-109).              */
 int pg_write_para_file(const pg_params *p, const char *path, const char *mainp);

@@ -121,7 +121,7 @@ def lib() -> C.CDLL:
         "pg_boundary_rings": (C.c_int, [P, C.POINTER(C.c_double), C.c_size_t, C.POINTER(C.c_int)]),
         "pg_label": (C.c_int, [P, C.c_char_p, C.c_size_t]),
         "pg_dump_name": (C.c_int, [P, C.c_char_p, C.c_int, C.c_char_p, C.c_size_t]),
-        "pg_write_time_rows": (C.c_int, [C.c_char_p, dp, C.c_int, C.c_int]),
+        "pg_write_time_rows": (C.c_int, [P, C.c_char_p, dp, C.c_int, C.c_int]),
         "pg_write_para_file": (C.c_int, [P, C.c_char_p, C.c_char_p]),
         "pg_create": (C.c_int, [P, C.c_int, C.POINTER(vp)]),
         "pg_destroy": (C.c_int, [vp]),

@@ -587,13 +587,16 @@ int pg_dump_name(const pg_params *p, const char *dir, int frame, char *buf, size
   return PG_OK;
 }
 
-int pg_write_time_rows(const char *path, const double *rows, int nrows, int append) {
-  if (!path || (!rows && nrows > 0) || nrows < 0) return PG_ERR_ARG;
+int pg_write_time_rows(const pg_params *p, const char *path, const double *rows, int nrows, int append) {
+  if (!p || !path || (!rows && nrows > 0) || nrows < 0) return PG_ERR_ARG;
   FILE *f = std::fopen(path, append ? "a" : "w");
   if (!f) return PG_ERR_IO;
+  // ofstream with precision(16) prints a double as %.16g; without a planet
+  // the row stops after the mass (main.cu:419-425)
+  const int ncols = p->plnt_flag > 0 ? 11 : 2;
   for (int r = 0; r < nrows; r++) {
     const double *q = rows + 11 * (size_t)r;
-    for (int c = 0; c < 11; c++) std::fprintf(f, c ? " %.16g" : "%.16g", q[c]);
+    for (int c = 0; c < ncols; c++) std::fprintf(f, c ? " %.16g" : "%.16g", q[c]);
     std::fputc('\n', f);
   }
   return std::fclose(f) == 0 ? PG_OK : PG_ERR_IO;

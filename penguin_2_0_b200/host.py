@@ -106,6 +106,26 @@ def label(p: pg_params) -> str:
     return b.value.decode()
 
 
+def dump_name(p: pg_params, directory: str, frame: int) -> str:
+    """<directory>/binary_<label>_<NNNNN>, the dump name of main.cu:124."""
+    b = C.create_string_buffer(4096)
+    _check(_lib.lib().pg_dump_name(C.byref(p), directory.encode(), int(frame), b, 4096), what="pg_dump_name")
+    return b.value.decode()
+
+
+def write_para_file(p: pg_params, path: str, mainp: str) -> None:
+    """read/para_<label>.dat as write_para_file (output.cu:90-109) writes it."""
+    _check(_lib.lib().pg_write_para_file(C.byref(p), path.encode(), mainp.encode()), what="pg_write_para_file")
+
+
+def write_time_rows(p: pg_params, path: str, rows, append: bool = False) -> None:
+    """files/time_<label>.dat rows (main.cu:417-427) from rows of 11 values in
+    the pg_history layout; two columns without a planet."""
+    a = np.ascontiguousarray(np.asarray(rows, dtype=np.float64).reshape(-1, 11))
+    _check(_lib.lib().pg_write_time_rows(C.byref(p), path.encode(), a.ctypes.data_as(C.POINTER(C.c_double)),
+                                         a.shape[0], int(append)), what="pg_write_time_rows")
+
+
 # ---- dump layout (variable_types.h:67-97) ---------------------------------------
 def dump_fields(buf, p: pg_params) -> dict:
     """Views of a dump image: r,p,u,v,w [nring, jmax] (storage order) and the

@@ -26,7 +26,7 @@ NULL_CALLS = {
     "pg_boundary_rings": ("L.pg_boundary_rings(C.byref(p), None, 0, None)", PG_ERR_ARG),
     "pg_label": ("L.pg_label(C.byref(p), None, 0)", PG_ERR_ARG),
     "pg_dump_name": ("L.pg_dump_name(C.byref(p), None, 0, None, 0)", PG_ERR_ARG),
-    "pg_write_time_rows": ("L.pg_write_time_rows(None, None, 1, 0)", PG_ERR_ARG),
+    "pg_write_time_rows": ("L.pg_write_time_rows(C.byref(p), None, None, 1, 0)", PG_ERR_ARG),
     "pg_write_para_file": ("L.pg_write_para_file(None, None, None)", PG_ERR_ARG),
     "pg_create": ("L.pg_create(C.byref(p), 0, None)", PG_ERR_ARG),
     "pg_destroy": ("L.pg_destroy(None)", PG_OK),
@@ -145,4 +145,4 @@ def test_undersized_buffers_are_refused():
     name = (C.c_char * 4)()
     assert L.pg_dump_name(C.byref(p), b"/tmp", 0, name, 4) == PG_ERR_ARG
     assert L.pg_label(C.byref(p), name, 2) == PG_ERR_ARG
-    assert L.pg_write_time_rows(b"/nonexistent-dir/t.dat", None, -1, 0) == PG_ERR_ARG
+    assert L.pg_write_time_rows(C.byref(p), b"/nonexistent-dir/t.dat", None, -1, 0) == PG_ERR_ARG

@@ -70,6 +70,7 @@ def main():
         xs = raw[:, 40 * p.jmax:40 * p.jmax + 32].copy().view(np.float64)
         ys = raw[0, 40 * p.jmax + 32:72 * p.jmax + 32].copy().view(np.float64).reshape(4, p.jmax)
         zs = raw[:, 72 * p.jmax + 32:72 * p.jmax + 64].copy().view(np.float64)
+        tail = raw[:, 72 * p.jmax + 64:72 * p.jmax + 96].copy()     # i k rot_v res_v rot_j inc_j
         b = np.fromfile(os.path.join(d, "boundary.bin"), dtype=np.uint8).reshape(-1, rb)
         bf = b[:, :40 * p.jmax].copy().view(np.float64).reshape(-1, 5, p.jmax)[:, :, 0]
         bx = b[:, 40 * p.jmax:40 * p.jmax + 32].copy().view(np.float64)
@@ -82,6 +83,7 @@ def main():
         out[f"{case}_phi_uniform"] = np.array(bool(np.all(f == f[:, :, :1])))
         out[f"{case}_xs"] = xs
         out[f"{case}_zs"] = zs
+        out[f"{case}_tail"] = tail
         out[f"{case}_ys"] = ys
         out[f"{case}_boundary"] = brec
         print(case, info, "boundary rings", brec.shape[0], flush=True)

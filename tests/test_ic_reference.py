@@ -6,7 +6,8 @@ init_speed, init_cells and init_bound produced on the host for four disks
 (tests/golden/make_ic_golden.py, oracle/ref/ic_harness.cu).  The library's
 initial dump (pg_build_ic without noise) and its boundary rings
 (pg_boundary_rings, the values a run loads into its ghost rows and polar
-ghost layers) agree with them bit for bit, with two exceptions:
+ghost layers) agree with them bit for bit, down to each ring record's i, k,
+res_v, rot_j and inc_j, with three exceptions:
 
 * v_r: the seeded initial state of this library starts at rest radially
   (v_r = 0); the reference's fresh start sets the viscous inflow speed
@@ -16,6 +17,9 @@ ghost layers) agree with them bit for bit, with two exceptions:
   then uses, so its Sigma, p, v_phi and rot_v there are left over from
   whatever the variables held; here they take the disk profile's values.
   Their geometry and v_r still agree.
+* rot_v: the reference's fresh start leaves it 0 until its first Index_Shift
+  (main.cu:330); the initial dump here is a restart file, which carries that
+  Index_Shift's value because a restart skips the call.
 
 The 3D interior state is the part of the 3D set-up that no reference run
 checks otherwise (the reference has no 3D sweep)."""
@@ -80,3 +84,35 @@ def test_boundary_rings_match_reference_setup(case):
             cols = [c for c in cols if c not in ("r", "p", "v", "rot_v")]
         for c in cols:
             np.testing.assert_array_equal(got[:, COL[c]], want[:, COL[c]], err_msg=f"{name}.{c}")
+
+
+@pytest.mark.parametrize("case", list(IC_CASES))
+def test_ring_record_tails_match_reference_setup(case):
+    """The per-ring integers and FARGO scalars of the dump (variable_types.h:
+    i, k, rot_v, res_v, rot_j, inc_j).  All agree bit for bit except rot_v:
+    the reference's fresh start leaves it 0 for its first Index_Shift
+    (main.cu:330) to fill, while this library's initial dump is the restart
+    file, whose rot_v is that Index_Shift's value val.v - FrRot xc
+    (orbital_advection.cu:22), because a restart skips it."""
+    p = ic_params(case)
+    p.noise_amp = 0.0
+    buf = pg.build_ic(p)
+    rb = 72 * p.jmax + 96
+    ours = np.frombuffer(bytes(buf), dtype=np.uint8).reshape(-1, rb)[:, 72 * p.jmax + 64:]
+    ref = G[f"{case}_tail"]
+    assert ours.shape == ref.shape
+
+    def split(t):
+        t = np.ascontiguousarray(t)
+        return (t[:, 0:8].copy().view(np.int32), t[:, 8:16].copy().view(np.float64)[:, 0],
+                t[:, 16:24].copy().view(np.float64)[:, 0], t[:, 24:32].copy().view(np.int32))
+
+    ik, rot_v, res_v, jj = split(ours)
+    rik, rrot_v, rres_v, rjj = split(ref)
+    np.testing.assert_array_equal(ik, rik)            # i, k
+    np.testing.assert_array_equal(res_v, rres_v)
+    np.testing.assert_array_equal(jj, rjj)            # rot_j, inc_j
+    assert np.all(rrot_v == 0.0)
+    f = pg.dump_fields(buf, p)
+    _, frrot = pg.init_planet(p)
+    np.testing.assert_array_equal(rot_v, f["v"][:, 0] - frrot * f["xc"])

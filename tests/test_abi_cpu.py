@@ -1,6 +1,7 @@
 """Host-side checks that need no GPU: the C ABI library loads and exports
 every symbol include/penguin_b200.h declares, parameter validation, the
 seeded initial condition and the dump layout."""
+import os
 import subprocess
 
 import numpy as np
@@ -19,6 +20,22 @@ def test_library_exports_every_header_symbol():
     out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
     for n in names:
         assert f" T {n}" in out, n
+
+
+def test_ctypes_signatures_match_header_parameter_counts():
+    """Every declaration in include/penguin_b200.h has ctypes argtypes with
+    as many parameters (a mismatch would pass arguments in the wrong slots)."""
+    import re
+    txt = open(os.path.join(os.path.dirname(_lib.LIB_PATH), "..", "include", "penguin_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    decls = re.findall(r"\b(pg_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", txt, flags=re.S)
+    assert len(decls) == len(_lib.exported_symbols())
+    L = _lib.lib()
+    for name, args in decls:
+        a = args.strip()
+        n = 0 if a in ("", "void") else len(a.split(","))
+        at = getattr(L, name).argtypes
+        assert at is not None and len(at) == n, (name, n, at)
 
 
 def test_ring_bytes_matches_reference_layout():

@@ -16,7 +16,11 @@
  *
  * Parity is pinned against the reference's own CUDA build (oracle/_ref,
  * built from the reference sources by oracle/ref/build_ref.sh and run on a
- * B200): the golden vectors in tests/golden/ were produced by it.
+ * B200): the golden vectors in tests/golden/ were produced by it.  Its host
+ * set-up (ghost rings, damping targets) and its planet functions are pinned
+ * bit for bit to the reference's own host code, run through
+ * oracle/ref/ic_harness.cu and oracle/ref/planet_harness.cu
+ * (tests/test_oracle_setup.py, tests/test_planet_reference.py).
  */
 #ifndef PG_ORACLE_H
 #define PG_ORACLE_H

@@ -25,7 +25,9 @@
 // caches it.  Make that first call before any stream capture begins.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
+#include <mutex>
 
 #include "../../include/penguin_b200.h"
 #include "pg_ppm.cuh"
@@ -35,12 +37,16 @@ namespace {
 static __device__ __align__(256) double g_ring_part[PG_NOALLOC_MAX_RINGS];
 static __device__ __align__(256) unsigned int g_done[1];
 
+// per device: the scratch symbols' addresses, looked up once.  ready is set
+// with release order after part and done, so a thread that sees it set (acquire)
+// also sees the pointers; the mutex keeps two first calls from looking up at once.
 struct Scratch {
-  bool ready;
+  std::atomic<bool> ready;
   double *part;
   unsigned int *done;
 };
 static Scratch g_scratch[64];
+static std::mutex g_setup_mu;
 
 __device__ __forceinline__ double tree1024(double *list) {
   for (int len = 1024; len > 1; len >>= 1) {
@@ -119,13 +125,15 @@ __global__ void __launch_bounds__(1024) k_reduce_noalloc(
 int setup_device(int dev) {
   if (dev < 0 || dev >= 64) return PG_ERR_ARG;
   Scratch &s = g_scratch[dev];
-  if (s.ready) return PG_OK;
+  if (s.ready.load(std::memory_order_acquire)) return PG_OK;
+  std::lock_guard<std::mutex> lock(g_setup_mu);
+  if (s.ready.load(std::memory_order_relaxed)) return PG_OK;
   void *a = nullptr, *b = nullptr;
   if (cudaGetSymbolAddress(&a, g_ring_part) != cudaSuccess) return PG_ERR_CUDA;
   if (cudaGetSymbolAddress(&b, g_done) != cudaSuccess) return PG_ERR_CUDA;
   s.part = (double *)a;
   s.done = (unsigned int *)b;
-  s.ready = true;
+  s.ready.store(true, std::memory_order_release);
   return PG_OK;
 }
 

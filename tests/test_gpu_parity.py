@@ -96,6 +96,35 @@ def test_fused_loop_equals_host_loop(gpu, eos):
 
 
 @pytest.mark.gpu
+def test_output_times_fused_loop_equals_host_loop(gpu):
+    """tmovie well below the end time (dt ~0.018 on this disk): both loops cut
+    dt to land on every output time, then go back to the step before the cut
+    (main.cu:361-366, 407-411).  The device loop halts at each output time for
+    the host to dump, and the next pg_advance resumes from there."""
+    p = _params(dict(imax=256, jmax=768))
+    p.tmovie = 0.05
+    ic = pg.build_ic(p)
+    nsteps = 12
+    with pg.Run(p, 0) as a, pg.Run(p, 0) as b:
+        a.load(ic)
+        b.load(ic)
+        n, simtime, dt, planet, FrRot = a.kernel_loop(nsteps)
+        assert n == nsteps and simtime > 2 * p.tmovie
+        b.clock_reset(0)
+        done, calls = 0, 0
+        while done < nsteps and calls < 4 * nsteps:
+            done += b.advance(nsteps - done)
+            calls += 1
+        assert done == nsteps and calls > 2          # it stopped at the output times
+        c, pl = b.clock()
+        assert c.simtime == simtime
+        assert c.dt == dt
+        fa, fb = pg.dump_fields(a.save(), p), pg.dump_fields(b.save(), p)
+        for fld in ("r", "p", "u", "v", "rot_j", "inc_j", "res_v", "rot_v"):
+            np.testing.assert_array_equal(fa[fld], fb[fld], err_msg=fld)
+
+
+@pytest.mark.gpu
 def test_graph_equals_stream_loop(gpu):
     p = _params(dict(imax=256, jmax=768))
     ic = pg.build_ic(p)

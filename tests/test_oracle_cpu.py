@@ -46,3 +46,29 @@ def test_idle_last_radial_chunk_is_reproduced():
     h, f = _run(p, 1)
     assert np.array_equal(f["u"][116:], ic["u"][116:])
     assert not np.array_equal(f["u"][:116], ic["u"][:116])
+
+
+def test_output_time_cuts_agree_between_the_oracle_loops():
+    """tmovie well below the end time: the C restart loop (orc_run_steps) and
+    the step-by-step loop the GPU parity tests drive (tests/_lockstep.py) cut
+    dt to land on every output time and return to the step before the cut
+    (main.cu:361-366, 407-411); they agree bit for bit, and the output times
+    are hit exactly."""
+    from tests._lockstep import OracleLoop
+    p = pg.params(0, imax=128, jmax=132, nprin=1)
+    p.tmovie = 0.05
+    n = 10
+    h, f = _run(p, n)
+    loop = OracleLoop(p, pg.build_ic(p))
+    dts = [loop.step()[0] for _ in range(n)]
+    g = loop.fields()
+    np.testing.assert_array_equal(h[:, 1], dts)
+    for k in ("r", "u", "v", "rot_j"):
+        np.testing.assert_array_equal(f[k], g[k], err_msg=k)
+    t = h[:, 0]
+    k = np.floor(t / p.tmovie + 1e-9)
+    cuts = np.nonzero(np.diff(k) > 0)[0] + 1          # steps that end on an output time
+    assert len(cuts) >= 2
+    np.testing.assert_allclose(t[cuts], k[cuts] * p.tmovie, rtol=1e-14)
+    # after a cut the step returns to the uncut dt's growth path
+    assert all(h[c + 1, 1] > h[c, 1] for c in cuts if c + 1 < n)

@@ -1,6 +1,7 @@
 """Host-side checks that need no GPU: the C ABI library loads and exports
 every symbol include/penguin_b200.h declares, parameter validation, the
 seeded initial condition and the dump layout."""
+import ctypes as C
 import os
 import subprocess
 
@@ -163,3 +164,14 @@ def test_isentropic_3d_ic_is_the_polytrope():
         above += int(np.sum(Z >= z0))
         np.testing.assert_allclose(sig[k, :, 0], want, rtol=1.1e-4)   # the seeded noise is 1e-4
     assert below > 0 and above > 0
+
+
+def test_write_ic_file_equals_build_ic_bytes(tmp_path):
+    """pg_write_ic writes the restart file binary_<label>_00000 that the
+    reference's restart path reads (main.cu:246-262): the same bytes as
+    pg_build_ic, ring after ring in the dump layout."""
+    for which, over in ((0, dict(imax=64, jmax=132)), (1, dict(imax=32, jmax=132, kmax=8))):
+        p = pg.params(which, **over)
+        path = str(tmp_path / f"ic_{which}.bin")
+        assert _lib.lib().pg_write_ic(C.byref(p), path.encode()) == 0
+        assert open(path, "rb").read() == bytes(pg.build_ic(p))

@@ -40,6 +40,28 @@ extern "C" {
  * constants into runtime values.  n_pad (6) and arrsize (128, so 116 interior
  * cells per pencil chunk) are fixed: the sweep results depend on that chunk
  * size (the viscosity stencil at chunk edges sees un-remapped neighbours).   */
+/* The reference configures itself with macros of these names (global.h:16-26,
+ * variable_types.h); a translation unit that includes its headers before this
+ * one would otherwise rename the fields.  Each is set aside for the struct
+ * and restored after it.  Such a unit sets fields with pg_params_set.      */
+#pragma push_macro("ndim")
+#undef ndim
+#pragma push_macro("flat_flag")
+#undef flat_flag
+#pragma push_macro("EOS")
+#undef EOS
+#pragma push_macro("plnt_flag")
+#undef plnt_flag
+#pragma push_macro("FrRot_flag")
+#undef FrRot_flag
+#pragma push_macro("kill_flag")
+#undef kill_flag
+#pragma push_macro("visc_flag")
+#undef visc_flag
+#pragma push_macro("FARGO_flag")
+#undef FARGO_flag
+#pragma push_macro("dump_flag")
+#undef dump_flag
 typedef struct pg_params {
   /* grid (variable_types.h:11-20) */
   int    ndim;            /* 2 (r-phi) or 3 (r-phi-theta)                      */
@@ -70,6 +92,15 @@ typedef struct pg_params {
                              geometry, forces, time step and reductions    */
   int    reserved[7];
 } pg_params;
+#pragma pop_macro("dump_flag")
+#pragma pop_macro("FARGO_flag")
+#pragma pop_macro("visc_flag")
+#pragma pop_macro("kill_flag")
+#pragma pop_macro("FrRot_flag")
+#pragma pop_macro("plnt_flag")
+#pragma pop_macro("EOS")
+#pragma pop_macro("flat_flag")
+#pragma pop_macro("ndim")
 
 /* Planet state, same fields and order as struct body (variable_types.h:26-37). */
 typedef struct pg_body {
@@ -109,6 +140,16 @@ int pg_config_params(int which, pg_params *p);
  * limit of 65535 blocks in y (imax, and jmax in 3D).  EOS 0 (isothermal)
  * and EOS 1 (isentropic, p = cs2 Sigma^gam / gam) run in 2D and 3D.        */
 int pg_check_params(const pg_params *p);
+
+/* Set or read one field by its name ("EOS", "imax", "sc_h", "seed", ...).
+ * For callers whose translation unit includes the reference's configuration
+ * headers: their flag macros (EOS, ndim, plnt_flag, FrRot_flag, kill_flag,
+ * visc_flag, FARGO_flag, dump_flag, flat_flag) make p->EOS unwritable there,
+ * while pg_params_set(p, "EOS", EOS) works.  Integer fields take integral
+ * values only; an unknown name or a non-integral value for an integer field
+ * gives PG_ERR_ARG and leaves the struct as it was.                        */
+int pg_params_set(pg_params *p, const char *name, double value);
+int pg_params_get(const pg_params *p, const char *name, double *value);
 
 /* Size in bytes of one hydr_ring record of the dump layout
  * (variable_types.h:67-97): 72*jmax + 96; 0 for jmax <= 0.                 */

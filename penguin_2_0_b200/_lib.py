@@ -122,6 +122,8 @@ def lib() -> C.CDLL:
         "pg_label": (C.c_int, [P, C.c_char_p, C.c_size_t]),
         "pg_dump_name": (C.c_int, [P, C.c_char_p, C.c_int, C.c_char_p, C.c_size_t]),
         "pg_write_time_rows": (C.c_int, [P, C.c_char_p, dp, C.c_int, C.c_int]),
+        "pg_params_set": (C.c_int, [P, C.c_char_p, C.c_double]),
+        "pg_params_get": (C.c_int, [P, C.c_char_p, dp]),
         "pg_write_para_file": (C.c_int, [P, C.c_char_p, C.c_char_p]),
         "pg_create": (C.c_int, [P, C.c_int, C.POINTER(vp)]),
         "pg_destroy": (C.c_int, [vp]),

@@ -7,6 +7,8 @@
 #include "pg_host.h"
 
 #include <cmath>
+#include <cstddef>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -620,6 +622,86 @@ int pg_label(const pg_params *p, char *buf, size_t len) {
   std::string s = pg::label(*p);
   if (s.size() + 1 > len) return PG_ERR_ARG;
   std::memcpy(buf, s.c_str(), s.size() + 1);
+  return PG_OK;
+}
+
+}  // extern "C"
+
+// ---- pg_params by field name ------------------------------------------------
+// A translation unit that includes the reference's configuration headers
+// cannot name the fields that share a name with its macros (EOS, ndim,
+// plnt_flag, ...); it sets them by name instead.
+namespace {
+struct ParamField {
+  const char *name;
+  size_t off;
+  char kind;   // 'i' int, 'd' double, 'u' uint64
+};
+#define PGF(n, k) {#n, offsetof(pg_params, n), k}
+const ParamField kParamFields[] = {
+    PGF(ndim, 'i'), PGF(imax, 'i'), PGF(jmax, 'i'), PGF(kmax, 'i'), PGF(flat_flag, 'i'),
+    PGF(bary_flag, 'i'), PGF(EOS, 'i'), PGF(plnt_flag, 'i'), PGF(FrRot_flag, 'i'),
+    PGF(kill_flag, 'i'), PGF(visc_flag, 'i'), PGF(FARGO_flag, 'i'), PGF(dump_flag, 'i'),
+    PGF(nlft, 'i'), PGF(nrgh, 'i'), PGF(nudr, 'i'), PGF(ntop, 'i'), PGF(ncycend, 'i'),
+    PGF(nprin, 'i'), PGF(ngeomx, 'i'), PGF(ngeomy, 'i'), PGF(ngeomz, 'i'), PGF(grspx, 'i'),
+    PGF(grspy, 'i'), PGF(grspz, 'i'), PGF(precision, 'i'),
+    PGF(p_alpha, 'd'), PGF(p_beta, 'd'), PGF(ss_alpha, 'd'), PGF(sc_h, 'd'), PGF(Sigma_0, 'd'),
+    PGF(M_p, 'd'), PGF(R_p, 'd'), PGF(t_growth, 'd'), PGF(rs_fac, 'd'), PGF(gam, 'd'),
+    PGF(courant, 'd'), PGF(endtime, 'd'), PGF(tmovie, 'd'), PGF(xmin, 'd'), PGF(xmax, 'd'),
+    PGF(ymin, 'd'), PGF(ymax, 'd'), PGF(zmin, 'd'), PGF(zmax, 'd'), PGF(dx_min, 'd'),
+    PGF(dx_max, 'd'), PGF(dy_min, 'd'), PGF(dy_max, 'd'), PGF(dz_min, 'd'), PGF(dz_max, 'd'),
+    PGF(noise_amp, 'd'), PGF(kill_rin, 'd'), PGF(kill_rout, 'd'),
+    PGF(seed, 'u'),
+};
+#undef PGF
+
+const ParamField *find_field(const char *name) {
+  for (const ParamField &f : kParamFields)
+    if (std::strcmp(f.name, name) == 0) return &f;
+  return nullptr;
+}
+}  // namespace
+
+extern "C" {
+
+int pg_params_set(pg_params *p, const char *name, double value) {
+  if (!p || !name) return PG_ERR_ARG;
+  const ParamField *f = find_field(name);
+  if (!f) return PG_ERR_ARG;
+  unsigned char *base = reinterpret_cast<unsigned char *>(p) + f->off;
+  if (f->kind == 'd') {
+    std::memcpy(base, &value, sizeof value);
+    return PG_OK;
+  }
+  if (!(value == std::floor(value))) return PG_ERR_ARG;            // integral, not NaN
+  if (f->kind == 'i') {
+    if (value < -2147483648.0 || value > 2147483647.0) return PG_ERR_ARG;
+    int v = (int)value;
+    std::memcpy(base, &v, sizeof v);
+  } else {
+    if (value < 0.0 || value > 9007199254740992.0) return PG_ERR_ARG;   // exact in a double
+    uint64_t v = (uint64_t)value;
+    std::memcpy(base, &v, sizeof v);
+  }
+  return PG_OK;
+}
+
+int pg_params_get(const pg_params *p, const char *name, double *value) {
+  if (!p || !name || !value) return PG_ERR_ARG;
+  const ParamField *f = find_field(name);
+  if (!f) return PG_ERR_ARG;
+  const unsigned char *base = reinterpret_cast<const unsigned char *>(p) + f->off;
+  if (f->kind == 'd') {
+    std::memcpy(value, base, sizeof(double));
+  } else if (f->kind == 'i') {
+    int v;
+    std::memcpy(&v, base, sizeof v);
+    *value = v;
+  } else {
+    uint64_t v;
+    std::memcpy(&v, base, sizeof v);
+    *value = (double)v;
+  }
   return PG_OK;
 }
 

@@ -21,6 +21,8 @@ NULL_CALLS = {
     "pg_default_params": ("L.pg_default_params(None)", PG_ERR_ARG),
     "pg_config_params": ("L.pg_config_params(0, None)", PG_ERR_ARG),
     "pg_check_params": ("L.pg_check_params(None)", PG_ERR_ARG),
+    "pg_params_set": ("L.pg_params_set(C.byref(p), None, 1.0)", PG_ERR_ARG),
+    "pg_params_get": ("L.pg_params_get(C.byref(p), b'EOS', None)", PG_ERR_ARG),
     "pg_write_ic": ("L.pg_write_ic(C.byref(p), None)", PG_ERR_ARG),
     "pg_build_ic": ("L.pg_build_ic(C.byref(p), None, 0)", PG_ERR_ARG),
     "pg_boundary_rings": ("L.pg_boundary_rings(C.byref(p), None, 0, None)", PG_ERR_ARG),

@@ -31,13 +31,15 @@ and pg_advance_graph (the ABI's replacement of main.cu's loop) run the steps,
 every step's diagnostics row (dt, mass, torque, ...) is read back (pg_history)
 and the final dump is saved to pinned host memory, all inside the timed
 region; after one untimed job the job runs three times and the median is
-reported.
+reported.  A job is E2E_STEPS = 200 steps whatever --steps is.
 e2e_host_loop times the reference's per-call sequence instead
 (pg_get_dt, pg_index_shift, pg_sweep2d/3d, pg_damp, pg_reduce from a Python
 loop with main.cu's host syncs: dt, planet and FrRot to the device, dt, mass
 and torque back every step).
-cpu_baseline: the CPU oracle (a restatement of the reference's sweeps in C,
-OpenMP over the box's cores) on a bounded sample of the same workload.
+cpu_baseline: the reference's own hydro step compiled for the host CPU
+(oracle/refhost: its .cu sources unchanged, one fiber per CUDA thread, OpenMP
+over the blocks) on a bounded sample of the same workload;
+cpu_baseline_port: the C restatement (oracle/pg_oracle.c) on the same sample.
 """
 from __future__ import annotations
 
@@ -55,6 +57,7 @@ sys.path.insert(0, ROOT)
 
 E2E_JOBS = 5      # e2e jobs timed; the median is reported
 E2E_WARM = 2      # untimed e2e jobs before them
+E2E_STEPS = 200   # steps of one e2e job, whatever --steps is
 
 WORKLOADS = {
     # name: (config index, overrides, description)
@@ -154,15 +157,17 @@ def _barrier(dist):
 
 
 def cpu_sample(p, steps: int, budget_s: float = 20.0):
-    """Time the CPU oracle on the same workload (bounded by budget_s)."""
+    """Time the CPU oracle (the C restatement) on the same workload (bounded
+    by budget_s); set-up happens before the clock starts."""
     import penguin_2_0_b200 as pg
     from oracle.pyoracle import Oracle
-    orc = Oracle(p, pg.build_ic(p))
+    ic = pg.build_ic(p)
+    orc = Oracle(p, ic)
     t0 = time.perf_counter()
     orc.run_steps(1)   # first step includes set-up effects
     one = time.perf_counter() - t0
     n = max(1, min(steps, int(budget_s / max(one, 1e-6))))
-    orc2 = Oracle(p, pg.build_ic(p))
+    orc2 = Oracle(p, ic)
     t0 = time.perf_counter()
     done = orc2.run_steps(n).shape[0]
     dt = time.perf_counter() - t0
@@ -170,52 +175,142 @@ def cpu_sample(p, steps: int, budget_s: float = 20.0):
     return cells * done / dt, done, Oracle.threads(), dt
 
 
-def run_reference(args):
-    """--impl reference: the reference's sweeps restated in C (the reference
-    itself only exists as CUDA), on the host cores, same workload and metric."""
-    dist, rank, ws = _dist()
-    if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
-        return
+def refhost_exe(workload: str, params: dict):
+    """The reference's own hydro step built for the host CPU for this
+    workload (oracle/refhost/build_bench.py; its grid and parameters are
+    compile-time), or None when it is absent or was built for other
+    parameters."""
+    d = os.path.join(ROOT, "oracle", "_ref", f"bench_{workload}")
+    exe = os.path.join(d, "penguin_ref_host")
+    if not os.path.exists(exe):
+        return None
+    try:
+        built = json.load(open(os.path.join(d, "params.json")))
+    except Exception:
+        return None
+    skip = {"precision"}
+    norm = lambda v: float.fromhex(v) if isinstance(v, str) and v.lstrip("-").startswith("0x") else v
+    same = all(norm(built.get(k)) == norm(v) for k, v in params.items() if k not in skip)
+    return exe if same else None
+
+
+def refhost_sample(exe: str, ic_path: str, budget_s: float, max_steps: int):
+    """Time the reference's own step loop built for the host (oracle/refhost):
+    a 1-step run sizes the sample, then a run of k steps; the binary times its
+    step loop on the host clock (loop_ms_total: get_dt, Index_Shift, planet,
+    bundle_sweep2D, damping, reductions), without its set-up.  OpenMP spreads
+    the CUDA blocks over every host core."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as out:
+        def go(n):
+            r = subprocess.run([exe, ic_path, str(n), out, ""], capture_output=True, text=True, check=True)
+            return json.loads(r.stdout.strip().splitlines()[-1])
+        one = go(1)
+        k = max(1, min(max_steps, int(budget_s / max(one["loop_ms_total"] / 1e3, 1e-6))))
+        d = go(k)
+    el = d["loop_ms_total"] / 1e3
+    cores = int(os.environ.get("OMP_NUM_THREADS", "0")) or os.cpu_count()
+    return d["cells"] * d["steps"] / el, d["steps"], cores, el
+
+
+REFHOST_3D_NOTE = ("the reference has no polar sweep (bundle_sweep3D is called at main.cu:376 and defined "
+                   "nowhere); its step on this 3D disk is bundle_sweep2D over every polar layer, two sweeps of "
+                   "our three, so this rate counts a lighter step than the GPU arm's")
+
+
+def workload_config(workload: str, desc: str, imax: int, jmax: int, kmax: int, ws: int, chunk: int) -> dict:
+    """The bench line's config dict, the same for both arms."""
+    l2_resident = workload in ("cfg0", "cfg0_fp32")
+    return {"workload": desc, "cells": imax * jmax * kmax, "imax": imax, "jmax": jmax, "kmax": kmax,
+            "parallelism": f"replicas{ws}",
+            "l2": "flushed between steps (512 MB write)" if l2_resident
+            else "working set larger than L2, CUDA graphs of %d steps" % chunk}
+
+
+def write_workload(outdir: str, workload: str) -> None:
+    """--write-ic: the workload's parameters (params.json, floats as hex) and
+    its seeded initial dump (ic.bin), written by the product library in a
+    process of their own, so that the reference arm's process never loads it."""
     import penguin_2_0_b200 as pg
-    from oracle.pyoracle import Oracle
-    which, over, desc = WORKLOADS[args.workload]
+    which, over, desc = WORKLOADS[workload]
     if which is None:
-        # batched workloads: the CPU restatement advances their first disk
+        # batched workloads: the CPU arm advances their first disk
         from penguin_2_0_b200 import ensemble as E
         p = E.draw_ensemble(1, seed=0)[0]
         p.precision = 0
         desc = f"{desc}: its first disk ({p.imax}x{p.jmax}) on the CPU"
     else:
         p = pg.params(which, **over)
-    p.nprin = 1
-    cells = p.imax * p.jmax * p.kmax
-    orc = Oracle(p, pg.build_ic(p))
-    if args.warmup:
-        orc.run_steps(min(args.warmup, 3))
+    p.nprin = 100
+    p.seed = 0
+    p.endtime = 1.0e9
+    p.tmovie = 1.0e9
+    d = {k: (float(v).hex() if isinstance(v, float) else v) for k, v in p.as_dict().items()}
+    json.dump({"params": d, "desc": desc}, open(os.path.join(outdir, "params.json"), "w"))
+    with open(os.path.join(outdir, "ic.bin"), "wb") as f:
+        f.write(pg.build_ic(p))
+
+
+def run_reference(args):
+    """--impl reference: the reference's own hydro step compiled for the host
+    CPU (oracle/refhost: its unmodified .cu sources, one fiber per CUDA
+    thread, OpenMP over the blocks) on the box's cores, same workload, metric
+    and config.  Where no host build exists for the workload, the C
+    restatement of its sweeps (oracle/pg_oracle.c) runs instead.  The
+    initial dump and the parameters come from a separate, untimed process
+    (write_workload); this process loads no product library, and only the
+    step loop is inside the timed region."""
+    # rank 0 alone runs the CPU arm (no process group: the arm has no collective)
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    import tempfile
+    from oracle.abi import pg_params
     budget = float(os.environ.get("PG_REF_BUDGET_S", "60"))
-    t0 = time.perf_counter()
-    orc2 = Oracle(p, pg.build_ic(p))
-    h = orc2.run_steps(1)
-    one = time.perf_counter() - t0
-    k = max(1, min(args.steps, int(budget / max(one, 1e-6))))
-    t0 = time.perf_counter()
-    orc3 = Oracle(p, pg.build_ic(p))
-    done = orc3.run_steps(k).shape[0]
-    el = time.perf_counter() - t0
-    v = cells * done / el
+    with tempfile.TemporaryDirectory() as tmp:
+        subprocess.check_call([sys.executable, os.path.abspath(__file__), "--write-ic", tmp,
+                               "--workload", args.workload])
+        meta = json.load(open(os.path.join(tmp, "params.json")))
+        ic_path = os.path.join(tmp, "ic.bin")
+        p = pg_params.from_dict(meta["params"])
+        desc = meta["desc"]
+        cells = p.imax * p.jmax * p.kmax
+        exe = refhost_exe(args.workload, meta["params"])
+        if exe is not None:
+            v, done, cores, el = refhost_sample(exe, ic_path, budget, args.steps)
+            kind = "reference"
+            sample = f"{done} steps of the {args.workload} disk (~{budget:g} s budget)"
+            if p.ndim == 3:
+                sample += "; " + REFHOST_3D_NOTE
+            note = ("the reference's own .cu sources compiled for the host (oracle/refhost): each CUDA thread a "
+                    "fiber, __syncthreads a yield, blocks over the host cores with OpenMP")
+        else:
+            from oracle.pyoracle import Oracle
+            ic = open(ic_path, "rb").read()
+            orc = Oracle(p, ic)
+            orc.run_steps(min(args.warmup, 3))
+            orc = Oracle(p, ic)
+            t0 = time.perf_counter()
+            orc.run_steps(1)
+            one = time.perf_counter() - t0
+            k = max(1, min(args.steps, int(budget / max(one, 1e-6))))
+            orc = Oracle(p, ic)
+            t0 = time.perf_counter()
+            done = orc.run_steps(k).shape[0]
+            el = time.perf_counter() - t0
+            v = cells * done / el
+            cores, kind = Oracle.threads(), "port"
+            sample = f"{done} full steps of the {args.workload} disk ({k} requested, ~{budget:g} s budget)"
+            note = ("no host build of the reference for this workload; this arm runs its restatement "
+                    "(oracle/pg_oracle.c) with OpenMP on the host cores")
     line = {
         "impl": "reference", "metric": "zone-updates/s", "value": v, "unit": "zone-updates/s",
         "n_gpus": args.gpus, "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / done,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic seeded disk (no public dataset)",
-        "config": {"workload": desc, "cells": cells, "sample": f"{done} steps of {k} requested"},
-        "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": Oracle.threads(), "kind": "port",
-                         "sample": f"{done} full steps of the {args.workload} disk"},
+        "data": "synthetic seeded disk (no public dataset), one independent disk per GPU",
+        "config": workload_config(args.workload, desc, p.imax, p.jmax, p.kmax, args.gpus, args.chunk),
+        "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference's hot path exists only as CUDA; this arm runs its restatement (oracle/pg_oracle.c) "
-                "with OpenMP on the host cores",
+        "note": note,
     }
     print(json.dumps(line))
 
@@ -370,7 +465,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--profile", action="store_true",
                     help="only W + K steps of the fused loop (stream launches), no extra legs; for ncu")
+    ap.add_argument("--write-ic", metavar="DIR", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.write_ic:
+        return write_workload(args.write_ic, args.workload)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -481,7 +579,7 @@ def main():
     # pg_index_shift, pg_sweep*, pg_damp, pg_reduce with main.cu's host syncs)
     # is timed the same way as e2e_host_loop.
     import numpy as np
-    e2e_steps = max(3, min(args.steps // 10, 200))
+    e2e_steps = E2E_STEPS
     dump_bytes = len(ic)
     pin_in = torch.empty(dump_bytes, dtype=torch.uint8, pin_memory=True)
     pin_in.numpy()[:] = np.frombuffer(bytes(ic), dtype=np.uint8)
@@ -540,11 +638,29 @@ def main():
     hl_value = cells * e2e_steps * ws / hl_el
     run3.close()
 
-    cpu = None
+    cpu = cpu_port = None
     if rank == 0 and not args.no_cpu:
-        v, done, cores, el = cpu_sample(p, 400, budget_s=float(os.environ.get("PG_CPU_BUDGET_S", "15")))
-        cpu = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "port",
-               "sample": f"{done} steps of the same disk in {el:.1f} s"}
+        budget = float(os.environ.get("PG_CPU_BUDGET_S", "15"))
+        pref = pg.params(None)
+        pref.update(**p.as_dict())
+        pref.seed = 0
+        d = {k: (float(v).hex() if isinstance(v, float) else v) for k, v in pref.as_dict().items()}
+        exe = refhost_exe(args.workload, d)
+        if exe is not None:
+            import tempfile
+            with tempfile.TemporaryDirectory() as tmp:
+                icp = os.path.join(tmp, "ic.bin")
+                open(icp, "wb").write(pg.build_ic(pref))
+                v, done, cores, el = refhost_sample(exe, icp, budget, 400)
+            cpu = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "reference",
+                   "sample": f"{done} steps of the same disk in {el:.1f} s, the reference's own sources built "
+                             f"for the host (oracle/refhost)" + ("; " + REFHOST_3D_NOTE if p.ndim == 3 else "")}
+        v, done, cores, el = cpu_sample(p, 400, budget_s=budget)
+        cpu_port = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "port",
+                    "sample": f"{done} full steps of the same disk in {el:.1f} s, the C restatement "
+                              f"(oracle/pg_oracle.c)"}
+        if cpu is None:
+            cpu, cpu_port = cpu_port, None
 
     if rank == 0:
         line = {
@@ -553,15 +669,13 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if p.precision == 1 else "f64",
             "data": "synthetic seeded disk (no public dataset), one independent disk per GPU",
-            "config": {"workload": desc, "cells": cells, "imax": p.imax, "jmax": p.jmax, "kmax": p.kmax,
-                       "parallelism": f"replicas{ws}",
-                       "l2": "flushed between steps (512 MB write)" if l2_resident
-                       else "working set larger than L2, CUDA graphs of %d steps" % args.chunk},
+            "config": workload_config(args.workload, desc, p.imax, p.jmax, p.kmax, ws, args.chunk),
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak,
                          "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "bytes_per_launch": bytes_per_launch,
                          "mean_launch_ms": mean[top], "kernels_ms": mean},
             "cpu_baseline": cpu,
+            "cpu_baseline_port": cpu_port,
             "e2e": {"value": e2e_value, "unit": "zone-updates/s",
                     "h2d_bytes_per_step": dump_bytes / e2e_steps,
                     "d2h_bytes_per_step": (dump_bytes + 8 * 11 * e2e_steps) / e2e_steps,

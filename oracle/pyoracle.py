@@ -1,7 +1,8 @@
 """ctypes binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
-module; the product path never imports it.  The oracle is built in-tree
+module; the product path never imports it, and it imports nothing of the
+product (its struct images are in oracle/abi.py).  The oracle is built in-tree
 by build() into oracle/liboracle.so (gcc + OpenMP).
 """
 from __future__ import annotations
@@ -37,8 +38,9 @@ def lib():
             build()
         L = C.CDLL(SO)
         vp, dp = C.c_void_p, C.POINTER(C.c_double)
-        from penguin_2_0_b200._lib import pg_body, pg_params
-        P, B = C.POINTER(pg_params), C.POINTER(pg_body)
+        # params and bodies go in by reference as plain pointers: the caller's
+        # struct may be oracle.abi's or the product binding's (same layout)
+        P, B = vp, vp
         sig = {
             "orc_create": (vp, [P, vp, C.c_size_t]),
             "orc_destroy": (None, [vp]),

@@ -1,15 +1,15 @@
 #!/bin/bash
 # Build the reference's own CUDA hydro step for one workload (oracle/_ref).
 #   oracle/ref/build_ref.sh <name> <params.json> [golden|perf]
-# Compiles the reference's translation units where they lie (read-only tree,
-# default /root/reference, override with PG_REFERENCE) against per-workload
+# Compiles the reference's translation units where they lie (the read-only
+# tree named by PG_REFERENCE, which must be set) against per-workload
 # copies of its two configuration headers (gen_headers.py) and links them
 # with ref_harness.cu.  Output: oracle/_ref/<name>/penguin_ref (git-ignored).
 set -euo pipefail
 NAME=$1
 PJSON=$2
 MODE=${3:-golden}
-REF=${PG_REFERENCE:-/root/reference}
+REF=${PG_REFERENCE:?set PG_REFERENCE to the reference source tree}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$HERE/../_ref/$NAME
 mkdir -p "$OUT/obj"

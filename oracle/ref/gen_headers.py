@@ -7,7 +7,7 @@ headers from the reference tree, substitutes the values of one parameter set
 the result to oracle/_ref/<name>/include/, which is git-ignored.  Nothing
 else of the reference is copied: its .cu sources are compiled where they lie.
 
-usage: python oracle/ref/gen_headers.py <params.json> <outdir> [reference_root]
+usage: python oracle/ref/gen_headers.py <params.json> <outdir> <reference_root>
 """
 import json
 import os
@@ -56,7 +56,7 @@ def patch_global(txt, p):
 
 def main():
     pjson, outdir = sys.argv[1], sys.argv[2]
-    root = sys.argv[3] if len(sys.argv) > 3 else "/root/reference"
+    root = sys.argv[3]
     raw = json.load(open(pjson))
     p = {k: (float.fromhex(v) if isinstance(v, str) and v.startswith(("0x", "-0x")) else v)
          for k, v in raw.items()}

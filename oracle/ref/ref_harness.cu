@@ -13,13 +13,23 @@
 //   * after bundle_sweep2D a wave-damping kernel acts on cells with
 //     r < h_kill_rin or r > h_kill_rout (the workload's damping zones);
 //   * after every step it records simtime, dt, mass (mode 0) and torque
-//     (mode 9, normalised as main.cu:421) and, after the listed steps, the
-//     full rings in the dump layout.
+//     (mode 9, normalised as main.cu:421), FrRot and the planet's y, x, vx,
+//     vy and m, and, after the listed steps, the full rings in the dump
+//     layout.
+// Built with ndim 3, bundle_sweep2D runs the radial and azimuthal sweeps of
+// every polar layer (sweepx takes the layer from blockIdx.y, ppm.cu:33;
+// sweepy folds it into the ring index, ppm.cu:168) and rotate_rings: a 3D
+// step without the polar sweep, which the reference never wrote.
+//
+// The same driver, with its launches rewritten, runs the reference built for
+// the host (oracle/refhost); it then prints the host-clock time of the step
+// loop (loop_ms_total) beside the sweeps' (sweep_ms_total).
 //
 // usage: penguin_ref <ic_dump> <nsteps> <outdir> <steps-to-save, comma separated> [nodiag]
 // (nodiag: skip the mass/torque reductions, for timing the sweeps; the token
 // "end" in the list saves the state after the last step as state_final.bin)
 #include <unistd.h>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -168,6 +178,7 @@ int main(int argc, char **argv)
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0); cudaEventCreate(&e1);
   float sweep_ms = 0.f;
+  const auto loop_t0 = std::chrono::steady_clock::now();
   for (int s = 0; s < nsteps && cont_simu; s++) {
     dt = get_dt(dt, set, FrRot);
     if (ncycle == ncycend) cont_simu = false;
@@ -204,7 +215,8 @@ int main(int argc, char **argv)
       torque = GPU_output_reduction(set, planet, 0.0, 9) / (M_p * M_p * pow(R_p, 1.0 - p_alpha + (p_beta - 1.0)) / (sc_h * sc_h));
       #endif
     }
-    fprintf(hf, "%d %a %a %a %a %a %a\n", s, simtime, dt_used, mass, torque, FrRot, planet.y);
+    fprintf(hf, "%d %a %a %a %a %a %a %a %a %a %a\n", s, simtime, dt_used, mass, torque, FrRot, planet.y,
+            planet.x, planet.vx, planet.vy, planet.m);
     if (s + 1 < 100000 && keep[s + 1]) {
       CudaSafeCall(cudaMemcpy(set[0].h_rings, set[0].rings, set[0].memsize, cudaMemcpyDeviceToHost));
       char nm[64];
@@ -214,6 +226,7 @@ int main(int argc, char **argv)
       of.close();
     }
   }
+  const double loop_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - loop_t0).count();
   fclose(hf);
   if (keep_end) {
     CudaSafeCall(cudaMemcpy(set[0].h_rings, set[0].rings, set[0].memsize, cudaMemcpyDeviceToHost));
@@ -221,7 +234,8 @@ int main(int argc, char **argv)
     save_cells(of, set);
     of.close();
   }
-  printf("{\"steps\": %d, \"cells\": %d, \"sweep_ms_total\": %.6f}\n", ncycle, imax * jmax * kmax, sweep_ms);
+  printf("{\"steps\": %d, \"cells\": %d, \"sweep_ms_total\": %.6f, \"loop_ms_total\": %.6f}\n", ncycle,
+         imax * jmax * kmax, sweep_ms, loop_ms);
   CudaSafeCall(cudaFree(set[0].rings));
   CudaSafeCall(cudaFreeHost(set[0].h_rings));
   CudaSafeCall(cudaFree(set[0].lft));

@@ -35,7 +35,7 @@ def main():
     from make_golden import to_json
     from penguin_2_0_b200 import _lib
     import ctypes as C
-    ref = os.environ.get("PG_REFERENCE", "/root/reference")
+    ref = os.environ["PG_REFERENCE"]   # the reference source tree (required)
     out = os.path.join(ROOT, "oracle", "_ref", "grid")
     os.makedirs(out, exist_ok=True)
     p = _lib.pg_params()

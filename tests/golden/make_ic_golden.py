@@ -44,7 +44,7 @@ def ic_params(case):
 
 def main():
     from make_golden import to_json
-    ref = os.environ.get("PG_REFERENCE", "/root/reference")
+    ref = os.environ["PG_REFERENCE"]   # the reference source tree (required)
     out = {}
     for case in IC_CASES:
         p = ic_params(case)

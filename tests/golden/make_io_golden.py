@@ -10,7 +10,7 @@ and runs it on the host, where it makes no CUDA call:
 * one time-file row of ROW_VALUES through the stream append_output_file opens
   (output.cu:25-34; main.cu:417-427), two columns without a planet.
 
-Needs the reference tree (PG_REFERENCE, default /root/reference) and nvcc; no
+Needs the reference tree (PG_REFERENCE) and nvcc; no
 GPU.  usage: python tests/golden/make_io_golden.py
 """
 import json
@@ -52,7 +52,7 @@ def io_params(case):
 
 def main():
     from make_golden import to_json
-    ref = os.environ.get("PG_REFERENCE", "/root/reference")
+    ref = os.environ["PG_REFERENCE"]   # the reference source tree (required)
     out = {"mainp": MAINP, "row_values": [v.hex() for v in ROW_VALUES], "cases": {}}
     for case in IO_CASES:
         p = io_params(case)

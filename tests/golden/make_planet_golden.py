@@ -6,7 +6,7 @@ and runs it on the host, where it makes no CUDA call: init_planet, then
 NSTEPS steps of kick (dt/2), drift (dt), kick (dt/2) (planet.cu:36-93) under
 seeded disk forces, recording the body, FrRot, get_ecc, get_E and set_M_p.
 
-Needs the reference tree (PG_REFERENCE, default /root/reference) and nvcc; no
+Needs the reference tree (PG_REFERENCE) and nvcc; no
 GPU.  usage: python tests/golden/make_planet_golden.py
 """
 import json
@@ -50,7 +50,7 @@ def forces(case):
 
 def main():
     from make_golden import to_json
-    ref = os.environ.get("PG_REFERENCE", "/root/reference")
+    ref = os.environ["PG_REFERENCE"]   # the reference source tree (required)
     out = {"nsteps": np.array(NSTEPS), "dt": np.array(DT)}
     for case in PLANET_CASES:
         p = planet_params(case)

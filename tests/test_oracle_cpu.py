@@ -72,3 +72,17 @@ def test_output_time_cuts_agree_between_the_oracle_loops():
     np.testing.assert_allclose(t[cuts], k[cuts] * p.tmovie, rtol=1e-14)
     # after a cut the step returns to the uncut dt's growth path
     assert all(h[c + 1, 1] > h[c, 1] for c in cuts if c + 1 < n)
+
+
+def test_oracle_struct_images_match_the_product_binding():
+    """oracle/abi.py keeps its own images of pg_params and pg_body so the CPU
+    baseline can run without the product library; they must be the product
+    binding's layout exactly (names, types, offsets, size)."""
+    import ctypes as C
+    from oracle import abi
+    from penguin_2_0_b200 import _lib
+    for mine, theirs in ((abi.pg_params, _lib.pg_params), (abi.pg_body, _lib.pg_body)):
+        assert C.sizeof(mine) == C.sizeof(theirs)
+        assert [(n, t) for n, t in mine._fields_] == [(n, t) for n, t in theirs._fields_]
+        for n, _ in mine._fields_:
+            assert getattr(mine, n).offset == getattr(theirs, n).offset, n

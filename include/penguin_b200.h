@@ -220,7 +220,9 @@ int pg_get_dt(pg_run *run, double dt_old, double frrot, double *dt_out);
 int pg_index_shift(pg_run *run, double dt, double frrot);
 
 /* bundle_sweep2D (ppm.cu:358-386): radial sweep, azimuthal sweep with the
- * FARGO integer shift applied at its store, rotate_rings.                 */
+ * FARGO integer shift applied at its store, rotate_rings.  On a 3D run it
+ * does what the reference's bundle_sweep2D does on a 3D build: those two
+ * sweeps over every polar layer and rotate_rings, without a polar sweep.  */
 int pg_sweep2d(pg_run *run, double dt, const pg_body *planet, double frrot);
 
 /* The 3D counterpart the reference calls at main.cu:376 but never defines:
@@ -312,14 +314,20 @@ int pg_timing_read(pg_run *run, double *ms_sum, int64_t *counts, int nkinds);
  * device arrays the caller owns: sigma[i*row_stride + j] in physical azimuth
  * order, per ring xc, xvol, rot_j, per column yc, yvol; *out is a device
  * double written by the kernel on `stream` (no host copy, no sync).  For
- * callers that must not allocate device memory (during graph capture, inside
- * a fixed memory pool, in a time loop that allocated everything up front):
+ * callers that must not allocate device memory (a process whose HBM belongs
+ * to its own memory pool, a time loop that allocated everything up front and
+ * wants no allocation or its implicit synchronisation inside the loop):
  * the entry point calls no cudaMalloc/cudaFree; its scratch is a static
  * __device__ array of PG_NOALLOC_MAX_RINGS doubles that every GPU loading the
  * library keeps until exit.  imax above that limit returns PG_ERR_PARAMS.
  * The first call on a device looks the array up with cudaGetSymbolAddress
  * (make it before any stream capture); calls share the array, so calls that
- * overlap on the GPU race.  Modes 8 and 9 assume a planet (plnt_flag > 0). */
+ * overlap on the GPU race.  Modes 8 and 9 assume a planet (plnt_flag > 0)
+ * and, as the reference, test the exclusion radius on the physical azimuth
+ * against planet->y without wrapping.  rot_j may be any int (it is reduced
+ * modulo jmax).  For imax <= 1024 the result equals the reference's
+ * summation order bit for bit; above that the ring partials are summed in
+ * 1024-wide blocks, an extension the reference's output_lv3 does not have. */
 #define PG_NOALLOC_MAX_RINGS 16384
 int pg_reduce_noalloc(const double *sigma, int64_t row_stride, const double *xc,
                       const double *xvol, const int *rot_j, const double *yc,

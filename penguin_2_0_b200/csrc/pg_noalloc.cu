@@ -2,14 +2,13 @@
 // device memory.
 //
 // Who needs it: callers that hold their own device buffers and must not
-// allocate.  Examples: a host thread that is capturing a CUDA graph (cudaMalloc
-// is not a stream operation and cannot be captured), a serving process that
-// has handed all of its HBM to its own memory pool, or a driver loop (such
-// as the reference's main.cu with its own GPU_plan buffers) that allocates
-// once at start-up and wants no allocation, or the implicit synchronisation
-// cudaMalloc may bring, inside its time loop.  pg_reduce needs a pg_run, whose
-// creation allocates; this entry point works on plain device pointers the
-// caller owns.
+// allocate.  Examples: a serving process that has handed all of its HBM to
+// its own memory pool (a cudaMalloc there fails or steals from the pool), or
+// a driver loop (such as the reference's main.cu with its own GPU_plan
+// buffers) that allocates once at start-up and wants no allocation, nor the
+// implicit device synchronisation cudaMalloc/cudaFree may bring, inside its
+// time loop.  pg_reduce needs a pg_run, whose creation allocates; this entry
+// point works on plain device pointers the caller owns.
 //
 // Scratch: the per-ring partial sums and the completion counter live in
 // file-scope __device__ arrays of fixed size, PG_NOALLOC_MAX_RINGS rings
@@ -59,7 +58,12 @@ __device__ __forceinline__ double tree1024(double *list) {
 
 // output_lv1 + output_lv3 of device_func.cu:49-167 (2D), over caller arrays:
 // sigma[i*row_stride + j] in physical azimuth order, rot_j[i] the ring's FARGO
-// offset (storage index j_s holds physical (j_s + rot_j) mod jmax).
+// offset (storage index j_s holds physical (j_s + rot_j) mod jmax).  rot_j
+// may be any int: it is reduced into [0, jmax) once per ring, which for the
+// offsets output_lv1 wraps (device_func.cu:71-73, -jmax < rot_j < 2 jmax)
+// gives the same column.  With imax <= 1024 the ring partials are summed in
+// output_lv3's single 1024-wide tree; above that they are summed 1024 at a
+// time, an extension with no reference counterpart (output_lv3 holds 1024).
 __global__ void __launch_bounds__(1024) k_reduce_noalloc(
     const double *sigma, long long row_stride, const double *xc, const double *xvol, const int *rot_j,
     const double *yc, const double *yvol, int imax, int jmax, pgd::Body pl, double exclude, int mode,
@@ -67,7 +71,8 @@ __global__ void __launch_bounds__(1024) k_reduce_noalloc(
   __shared__ double list[1024];
   __shared__ bool is_last;
   const int i = blockIdx.x, tt = threadIdx.x;
-  const int rot = rot_j[i];
+  int rot = rot_j[i] % jmax;
+  if (rot < 0) rot += jmax;
   const double rad = xc[i], xv = xvol[i];
   const double *row = sigma + (size_t)i * row_stride;
   const int loop = jmax / 1024 + (jmax % 1024 != 0);

@@ -564,21 +564,25 @@ static int nx(pg_run *run) { return pgk::sweep_launches(run->T.cx); }
 static int ny(pg_run *run) { return pgk::sweep_launches(run->T.cy); }
 static int nz(pg_run *run) { return pgk::sweep_launches(run->T.cz); }
 
+// On a 3D run this is what the reference's bundle_sweep2D does on a 3D
+// build: the radial and azimuthal sweeps of every polar layer (sweepx takes
+// the layer from blockIdx.y, ppm.cu:33; sweepy folds it into the ring index,
+// ppm.cu:168) and rotate_rings, with no polar sweep.
 int pg_sweep2d(pg_run *run, double dt, const pg_body *planet, double frrot) {
   if (!run || !planet) return PG_ERR_ARG;
   if (!run->loaded) return fail(run, PG_ERR_STATE, "no state loaded");
-  if (run->P.ndim != 2) return fail(run, PG_ERR_PARAMS, "pg_sweep2d on a 3D run");
   CK(cudaSetDevice(run->dev));
   pgd::SweepCtl c = host_ctl(dt, planet, frrot);
   cudaStream_t s = run->stream;
+  const int nd = run->P.ndim;
   if (run->fp32) {
-    pgk::sweep_x32(run->T, planes32_fwd(run, run->cur), run->ph, c, 2, s);
+    pgk::sweep_x32(run->T, planes32_fwd(run, run->cur), run->ph, c, nd, s);
     c.shift = 1;
-    pgk::sweep_y32(run->T, planes32_fwd(run, 1 - run->cur), run->ph, c, 2, s);
+    pgk::sweep_y32(run->T, planes32_fwd(run, 1 - run->cur), run->ph, c, nd, s);
   } else {
-    pgk::sweep_x(run->T, planes_fwd(run, run->cur, run->p0_live ? run->p0 : nullptr), run->ph, c, 2, s);
+    pgk::sweep_x(run->T, planes_fwd(run, run->cur, run->p0_live ? run->p0 : nullptr), run->ph, c, nd, s);
     c.shift = 1;
-    pgk::sweep_y(run->T, planes_fwd(run, 1 - run->cur, nullptr), run->ph, c, 2, s);
+    pgk::sweep_y(run->T, planes_fwd(run, 1 - run->cur, nullptr), run->ph, c, nd, s);
   }
   if (run->P.FARGO_flag > 0) pgk::rotate(run->T, nullptr, s);
   run->p0_live = false;

@@ -298,10 +298,13 @@ class Run:
         return np.frombuffer(buf, dtype=np.float64)[: n.value * HIST_COLS].reshape(n.value, HIST_COLS).copy()
 
     # ---- host-driven loop with the reference's call sequence ----
-    def kernel_loop(self, nsteps: int, startat: int = 0, damping: bool = True, record=None):
+    def kernel_loop(self, nsteps: int, startat: int = 0, damping: bool = True, record=None,
+                    sweep2d: bool = False):
         """main.cu:270-441 restart path, host-driven: one get_dt (host sync),
         Index_Shift, kick, bundle_sweep2D, damping, drift/forces/kick per step.
-        record(step, simtime, dt_used, planet, FrRot) is called after each step."""
+        record(step, simtime, dt_used, planet, FrRot) is called after each step.
+        A 3D run steps with bundle_sweep3D, or with bundle_sweep2D (radial and
+        azimuthal sweeps of every layer, no polar sweep) when sweep2d is set."""
         p = self.p
         dt = p.endtime
         simtime = p.tmovie * startat
@@ -330,7 +333,7 @@ class Run:
             Index_Shift(self, dt, FrRot)
             if p.plnt_flag > 0:
                 FrRot = kick_drift_kick(p, planet, FrRot, 0.5 * dt, True)
-            if p.ndim == 2:
+            if p.ndim == 2 or sweep2d:
                 bundle_sweep2D(self, dt, planet, FrRot)
             else:
                 bundle_sweep3D(self, dt, planet, FrRot)

@@ -54,6 +54,17 @@ def patch_global(txt, p):
     return txt
 
 
+def patch_post_global(txt, p):
+    """include/post_global.h (the read/ tools' configuration): dims and M_p."""
+    txt = re.sub(r"#define ndim \d+", f"#define ndim {p['ndim']}", txt)
+    for name in ("imax", "jmax", "kmax"):
+        txt, n = re.subn(rf"const int {name} = [^;]*;", f"const int {name} = {p[name]};", txt)
+        assert n == 1, name
+    txt, n = re.subn(r"const sdp M_p = [^;]*;", f"const sdp M_p = {fx(p['M_p'])};", txt)
+    assert n == 1
+    return txt
+
+
 def main():
     pjson, outdir = sys.argv[1], sys.argv[2]
     root = sys.argv[3]
@@ -66,6 +77,10 @@ def main():
     gl = open(os.path.join(root, "include", "global.h")).read()
     open(os.path.join(inc, "variable_types.h"), "w").write(patch_variable_types(vt, p))
     open(os.path.join(inc, "global.h"), "w").write(patch_global(gl, p))
+    # read/'s configuration header: grid sizes and the planet mass
+    pg_path = os.path.join(root, "include", "post_global.h")
+    if os.path.exists(pg_path):
+        open(os.path.join(inc, "post_global.h"), "w").write(patch_post_global(open(pg_path).read(), p))
     # harness-only constants (damping zones of the workload)
     with open(os.path.join(inc, "harness_params.h"), "w") as f:
         f.write("#pragma once\n")

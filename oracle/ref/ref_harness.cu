@@ -10,6 +10,8 @@
 // main.cu:343-441, with these harness changes:
 //   * the ghost rings lft/rgh are allocated zeroed, so their res_v/inc_j
 //     are 0 (the reference relies on fresh heap pages for that);
+//   * on 3D grids the inner radial ghost rings' fields may come from a file
+//     (see below: the reference leaves them unset);
 //   * after bundle_sweep2D a wave-damping kernel acts on cells with
 //     r < h_kill_rin or r > h_kill_rout (the workload's damping zones);
 //   * after every step it records simtime, dt, mass (mode 0) and torque
@@ -159,6 +161,27 @@ int main(int argc, char **argv)
   init_den(val);
   init_speed(val);
   init_bound(lft, rgh, udr, top);
+  // On a 3D spherical grid init_bound never forms the density and pressure
+  // of the inner radial ghost rings (init.cpp:289-294): their r, p, v and
+  // rot_v are whatever an earlier loop iteration left, and the radial sweep
+  // then fills the first rings of every layer with NaN.  When <ic_dump>.lft
+  // exists the harness takes r, p, u, v, w, rot_v of those rings from it
+  // (n_pad * kmax records of 6 doubles, ring i + n_pad k, phi-uniform).
+  {
+    string lp = string(icpath) + ".lft";
+    FILE *lf = fopen(lp.c_str(), "rb");
+    if (lf) {
+      for (int n = 0; n < n_pad * kmax; n++) {
+        double v[6];
+        if (fread(v, sizeof(double), 6, lf) != 6) { fprintf(stderr, "short %s\n", lp.c_str()); return 3; }
+        for (int j = 0; j < jmax; j++) {
+          lft[n].r[j] = v[0]; lft[n].p[j] = v[1]; lft[n].u[j] = v[2]; lft[n].v[j] = v[3]; lft[n].w[j] = v[4];
+        }
+        lft[n].rot_v = v[5];
+      }
+      fclose(lf);
+    }
+  }
   CudaSafeCall(cudaMemcpy(set[0].rings, set[0].h_rings, set[0].memsize, cudaMemcpyHostToDevice));
   CudaSafeCall(cudaMemcpy(set[0].lft, lft, n_pad * kmax * sizeof(hydr_ring), cudaMemcpyHostToDevice));
   CudaSafeCall(cudaMemcpy(set[0].rgh, rgh, n_pad * kmax * sizeof(hydr_ring), cudaMemcpyHostToDevice));

@@ -19,8 +19,9 @@ def rel_linf(a, b):
 class OracleLoop:
     """main.cu restart loop on the oracle, advanced one step per call."""
 
-    def __init__(self, p, ic):
+    def __init__(self, p, ic, sweep2d=False):
         self.p = p
+        self.sweep2d = sweep2d        # 3D: radial + azimuthal sweeps only (bundle_sweep2D)
         self.o = Oracle(p, ic)
         self.planet = pg_body()
         fr = C.c_double(0.0)
@@ -50,7 +51,10 @@ class OracleLoop:
         if p.plnt_flag > 0:
             olib().orc_kick_drift_kick(C.byref(p), C.byref(self.planet), C.byref(fr), 0.5 * dt, 1)
             self.FrRot = fr.value
-        o.sweep(dt, self.planet, self.FrRot)
+        if self.sweep2d:
+            olib().orc_sweep2d(o._h, dt, C.byref(self.planet), self.FrRot)
+        else:
+            o.sweep(dt, self.planet, self.FrRot)
         o.damp(dt)
         self.simtime += dt
         self.timem += dt

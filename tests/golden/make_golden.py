@@ -1,9 +1,11 @@
 """Golden vectors from the reference's own CUDA build.
 
-Three stages:
+Three stages (2D cases in CASES, 3D cases in CASES3D):
   build  (CPU container): write each case's parameter JSON and build
          oracle/_ref/<case>/penguin_ref from the reference sources
-         (oracle/ref/build_ref.sh).
+         (oracle/ref/build_ref.sh), and, for the per-step cases, the same
+         sources for the host CPU (oracle/_ref/<case>/penguin_ref_host,
+         oracle/refhost/build_refhost.sh).
   run    (on a B200): write each case's seeded initial dump with the library
          (pg_write_ic) and run the reference binary on it; raw output goes to
          <outdir>/<case>/ (hist.txt and state_NNNNN.bin in the dump layout).
@@ -57,7 +59,27 @@ CASES = {
     # frame rotating at the orbit of a planet at R_p = 0.3 (FrRot = 6.1) every
     # ring moves by whole cells each step
     "g136x136_fargo2": (0, dict(imax=136, jmax=136, FARGO_flag=2, R_p=0.3), 8, (1, 8)),
+    # plnt_flag 2, the reference's default (global.h:20): the planet moves
+    # under the disk's forces, summed by the mode 8/9 reductions
+    # (device_func.cu:83-108) in planet_forces (planet.cu:54-93)
+    "g136x136_moving": (0, dict(imax=136, jmax=136, plnt_flag=2), 8, (1, 4, 8)),
 }
+
+# 3D spherical disks (ndim 3, ngeom 2/4/5) on which the reference build runs
+# bundle_sweep2D: the radial and azimuthal sweeps of every polar layer and
+# rotate_rings, a 3D step without the polar sweep (the reference has none).
+# Same tuple as CASES; the fixture keeps Sigma, v_r, v_phi and v_theta of
+# every STRIDE3D-th cell.
+CASES3D = {
+    # the 128x1024x32 disk's physics (p_alpha 1.5, q = 3e-4, theta over 3h
+    # above the midplane) on 136 x 136 x 8, damping zones r < 0.6, r > 1.8
+    "g3d136x136x8": (1, dict(imax=136, jmax=136, kmax=8, kill_rin=0.6, kill_rout=1.8), 6, (1, 6)),
+    # isentropic EOS 1, gam 1.4, on a polar range inside the polytrope's
+    # height (theta over 1.4h above the midplane)
+    "g3d136x136x8_eos1": (1, dict(imax=136, jmax=136, kmax=8, EOS=1, gam=1.4, zmin=0.5 * 3.141592653589793 - 0.07),
+                          6, (1, 6)),
+}
+STRIDE3D = 7
 
 
 # Whole runs to the end time (the workload's 10 orbits): name -> (base
@@ -66,6 +88,9 @@ CASES = {
 # the 256 x 768 disk (see above).
 LONG_CASES = {
     "g252x780_10orbits": (0, dict(imax=252, jmax=780), 6000),
+    # q = 3e-5 (q/h^3 = 0.24) opens no gap: the reference's own 1-ulp
+    # sensitivity stays small, so the flat 1e-8 bound applies to the torque
+    "g252x780_10orbits_q3e-5": (0, dict(imax=252, jmax=780, M_p=3e-5), 6000),
 }
 
 
@@ -80,7 +105,12 @@ PERF_CASES = {
 
 def params_for(case):
     from penguin_2_0_b200 import _lib
-    base, over, *_ = CASES[case] if case in CASES else (LONG_CASES[case] if case in LONG_CASES else PERF_CASES[case])
+    for table in (CASES, CASES3D, LONG_CASES, PERF_CASES):
+        if case in table:
+            base, over, *_ = table[case]
+            break
+    else:
+        raise KeyError(case)
     p = _lib.pg_params()
     st = _lib.lib().pg_config_params(base, C.byref(p))
     assert st == 0
@@ -101,7 +131,7 @@ def _cases(names):
 
 
 def cmd_build():
-    for case in _cases(list(CASES) + list(PERF_CASES) + list(LONG_CASES)):
+    for case in _cases(list(CASES) + list(CASES3D) + list(PERF_CASES) + list(LONG_CASES)):
         p = params_for(case)
         d = os.path.join(ROOT, "oracle", "_ref", case)
         os.makedirs(d, exist_ok=True)
@@ -109,6 +139,9 @@ def cmd_build():
         json.dump(to_json(p), open(pj, "w"), indent=1)
         mode = "perf" if case in PERF_CASES else "golden"
         subprocess.check_call([os.path.join(ROOT, "oracle", "ref", "build_ref.sh"), case, pj, mode])
+        if case in CASES or case in CASES3D:
+            # the same sources built for the host CPU (tests/test_refhost_cpu.py)
+            subprocess.check_call([os.path.join(ROOT, "oracle", "refhost", "build_refhost.sh"), case])
 
 
 def cmd_perf(rawdir):
@@ -135,16 +168,31 @@ def cmd_perf(rawdir):
         print(json.dumps(d), flush=True)
 
 
+def write_ghost_override(p, icpath):
+    """<ic>.lft for a 3D case: r, p, u, v, w, rot_v of the inner radial ghost
+    rings (ring i + 6 k) as the library sets them (pg_boundary_rings).  The
+    reference's init_bound leaves them unset on a 3D spherical grid
+    (init.cpp:289-294), so its radial sweep would fill the first rings of
+    every layer with NaN; the harness loads them from this file."""
+    if p.ndim != 3:
+        return
+    import penguin_2_0_b200 as pg
+    lft = pg.host.boundary_rings(p)["lft"]
+    cols = [pg.host.BOUNDARY_FIELDS.index(c) for c in ("r", "p", "u", "v", "w", "rot_v")]
+    np.ascontiguousarray(lft[:, cols], dtype=np.float64).tofile(icpath + ".lft")
+
+
 def cmd_run(rawdir):
     from penguin_2_0_b200 import _lib
     L = _lib.lib()
-    for case in _cases(CASES):
-        _, _, nsteps, keep = CASES[case]
+    for case in _cases(list(CASES) + list(CASES3D)):
+        _, _, nsteps, keep = CASES[case] if case in CASES else CASES3D[case]
         p = params_for(case)
         out = os.path.join(rawdir, case)
         os.makedirs(out, exist_ok=True)
         ic = os.path.join(out, "ic.bin")
         assert L.pg_write_ic(C.byref(p), ic.encode()) == 0
+        write_ghost_override(p, ic)
         exe = os.path.join(ROOT, "oracle", "_ref", case, "penguin_ref")
         t0 = time.time()
         try:
@@ -236,7 +284,26 @@ def read_rings(path, p):
     return f, rot_j
 
 
+def cmd_pack3d(rawdir, outdir=HERE):
+    """3D fixtures: per-step history and, at the kept steps, Sigma, v_r,
+    v_phi, v_theta [4, every STRIDE3D-th cell of the rings in storage
+    order] plus rot_j of every ring."""
+    for case in _cases(CASES3D):
+        _, _, nsteps, keep = CASES3D[case]
+        p = params_for(case)
+        src = os.path.join(rawdir, case)
+        out = {"hist": _hist(os.path.join(src, "hist.txt")), "stride": np.array(STRIDE3D)}
+        for s in keep:
+            f, rot_j = read_rings(os.path.join(src, f"state_{s:05d}.bin"), p)
+            sel = f[:, [0, 2, 3, 4], :].transpose(1, 0, 2).reshape(4, -1)
+            out[f"fields_{s}"] = sel[:, ::STRIDE3D].copy()
+            out[f"rot_j_{s}"] = rot_j
+        np.savez_compressed(os.path.join(outdir, f"{case}.npz"), **out)
+        print("packed", case)
+
+
 def cmd_pack(rawdir, outdir=HERE, full=None):
+    cmd_pack3d(rawdir, outdir)
     for case in _cases(CASES):
         _, _, nsteps, keep = CASES[case]
         p = params_for(case)

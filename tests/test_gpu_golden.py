@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import penguin_2_0_b200 as pg
-from tests._golden import CASES, TOL, field_errors, load, params_for
+from tests._golden import CASES, TOL, check_planet, field_errors, load, params_for
 from tests._lockstep import torque_abs_scale
 
 
@@ -24,6 +24,8 @@ def test_host_loop_matches_reference_build(gpu, case):
         assert abs(simtime - h[0]) <= TOL * h[0]
         mass = pg.GPU_output_reduction(run, planet, 0.0, 0)
         assert abs(mass - h[2]) <= TOL * h[2], (step, mass, h[2])
+        if h.size > 6:
+            check_planet(step, planet, FrRot, h)
         if p.plnt_flag or step in keep:
             f = pg.dump_fields(run.save(), p)
             if p.plnt_flag:
@@ -42,7 +44,7 @@ def test_host_loop_matches_reference_build(gpu, case):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["g136x136", "g252x780", "g136x200_eos1", "g136x136_fargo2"])
+@pytest.mark.parametrize("case", ["g136x136", "g252x780", "g136x200_eos1", "g136x136_fargo2", "g136x136_moving"])
 def test_fused_loop_matches_reference_build(gpu, case):
     _, _, nsteps, keep = CASES[case]
     p = params_for(case)
@@ -58,8 +60,11 @@ def test_fused_loop_matches_reference_build(gpu, case):
             e = field_errors(f, g, s)
             assert max(e) <= TOL, (case, s, e)
         hist = run.history()
+        c, pl = run.clock()
     # one diagnostics row per step (nprin = 1): mass and torque of every step
     for s in range(max(keep)):
         h = g["hist"][s]
         assert abs(hist[s, 0] - h[0]) <= TOL * h[0]
         assert abs(hist[s, 1] - h[2]) <= TOL * h[2]
+    if g["hist"].shape[1] > 6:
+        check_planet(max(keep), pl, c.frrot, g["hist"][max(keep) - 1])

@@ -115,7 +115,8 @@ __device__ __forceinline__ double centre_force(int n, double dt, double rad, dou
 // (and w when THREED) hold the Lagrange-remapped values for 6 <= n < nmax-6.
 template <int AXIS, bool SPH, bool THREED, int EOS = 0, class SHM>
 __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, double FrRot,
-                                          const CellIn &c, const Body &pl, const Phys &ph) {
+                                          const CellIn &c, const Body &pl, const Phys &ph,
+                                          const double *eul_par = nullptr) {
   const bool act = n < nmax;
   double flat = 0.0;
   if (act) { S.q[n] = 0.0; S.dx[n] = 0.0; S.umid[n] = 0.0; S.pmid[n] = 0.0; S.tmp1[n] = 0.0; }
@@ -146,16 +147,28 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   }
 
   // ---- states states.cu:3-73 ----
-  // al = q, da = dx, a6 = tmp1, cs = umid, csfac = pmid (ppmlr.cu:30-33).
-  // paraset runs per cell as in the reference: tabulating its Eulerian
-  // coefficients in a separate kernel changes their FMA contraction (the
-  // last bits), which then shows up at 1e-12 in v_r.
+  // paraset's temporaries a/ai/b live in q/dx/tmp1; cs = umid, csfac = pmid
+  // (ppmlr.cu:30-33).  paraset runs per cell as in the reference:
+  // tabulating its Eulerian coefficients in a separate kernel changes their
+  // FMA contraction (the last bits), which then shows up at 1e-12 in v_r.
+  // The three parabolas of p, rho and u (states.cu:40-64) run side by side
+  // (parabola_n), with al/da/a6 in q/dx/tmp1 for p, s0/s1/s2 for rho and
+  // s3/s4/s5 for u; each value is the reference's, only the barriers are
+  // shared.
   const double hdt = 0.5 * dt;
   Par par;
-  paraset(n, 0, nmax, par, S.dx0, S.q, S.dx, S.tmp1);
+  if (AXIS == 2 && eul_par) {
+    // the polar sweep's Eulerian coefficients, one set per layer (k_tables;
+    // the polar sweep has no reference kernel whose bits it must follow)
+    if (n >= 1 && n < nmax - 1) {
+      const double *q = eul_par + 5 * n;
+      par.c0 = q[0]; par.c1 = q[1]; par.c2 = q[2]; par.c3 = q[3]; par.c4 = q[4];
+    }
+  } else {
+    paraset(n, 0, nmax, par, S.dx0, S.q, S.dx, S.tmp1);
+  }
   double ftot = 0.0;
   if (n >= 2 && n < nmax - 1) face_force<AXIS, SPH>(n, hdt, c, S, pl, ph, ftot);
-  __syncthreads();
   if (act) {
     double cs = hdt * sqrt(ph.gam * S.p[n] / S.r[n]) / S.dx0[n];
     if (AXIS == 1) cs /= c.rad;
@@ -163,57 +176,51 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
     S.umid[n] = cs;
     S.pmid[n] = 1.0 - kFourthd * cs;
   }
-  double spl = 0.0, spr = 0.0, srl = 0.0, srr = 0.0, sul = 0.0, sur = 0.0;
-  const double *cs = S.umid, *csfac = S.pmid;
-  double *al = S.q, *da = S.dx, *a6 = S.tmp1;
-  parabola(n, 0, nmax, flat, S.p, al, da, a6, par);
-  if (n >= 3 && n < nmax - 2) {
-    double t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
-    spl = fmax(kSmallp, t);
-    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
-    spr = fmax(kSmallp, t);
-  }
-  __syncthreads();
-  parabola(n, 0, nmax, flat, S.r, al, da, a6, par);
-  if (n >= 3 && n < nmax - 2) {
-    double t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
-    srl = fmax(kSmallr, t);
-    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
-    srr = fmax(kSmallr, t);
-  }
-  __syncthreads();
-  parabola(n, 0, nmax, flat, S.u, al, da, a6, par);
-  if (n >= 3 && n < nmax - 2) {
-    double t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
-    sul = t + hdt * ftot;
-    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
-    sur = t + hdt * ftot;
-  }
-  __syncthreads();
+  {
+    const double *val[3] = {S.p, S.r, S.u};
+    double *const al[3] = {S.q, S.s0, S.s3};
+    double *const da[3] = {S.dx, S.s1, S.s4};
+    double *const a6[3] = {S.tmp1, S.s2, S.s5};
+    parabola_n<3>(n, 0, nmax, flat, val, al, da, a6, par);
+    const double *cs = S.umid, *csfac = S.pmid;
+    double sl[3] = {0.0, 0.0, 0.0}, sr[3] = {0.0, 0.0, 0.0};
+    if (n >= 3 && n < nmax - 2) {
+#pragma unroll
+      for (int f = 0; f < 3; f++) {
+        sl[f] = al[f][n - 1] + da[f][n - 1] - cs[n - 1] * (da[f][n - 1] - csfac[n - 1] * a6[f][n - 1]);
+        sr[f] = al[f][n] + cs[n] * (da[f][n] + csfac[n] * a6[f][n]);
+      }
+    }
+    // riemann below writes umid/pmid, which hold cs/csfac read above
+    __syncthreads();
 
-  // ---- riemann riemann.cu:3-115, isothermal (45-53) or isentropic (75-111) ----
-  if (n >= 3 && n < nmax - 2) {
-    if (EOS == 0) {
-      double t1 = 0.5 * (sqrt(spl / srl) + sqrt(spr / srr));
-      double t2 = -0.5 * (sur - sul) / t1;
-      double pm = sqrt(spl * spr) * exp(t2);
-      S.umid[n] = sul - t1 * log(pm / spl);
-      S.pmid[n] = fmax(kSmallp, pm);
-    } else {
-      double um, pm;
-      riemann_isentropic(spl, srl, sul, spr, srr, sur, ph, um, pm);
-      S.umid[n] = um;
-      S.pmid[n] = pm;
+    // ---- riemann riemann.cu:3-115, isothermal (45-53) or isentropic (75-111) ----
+    if (n >= 3 && n < nmax - 2) {
+      const double spl = fmax(kSmallp, sl[0]), spr = fmax(kSmallp, sr[0]);
+      const double srl = fmax(kSmallr, sl[1]), srr = fmax(kSmallr, sr[1]);
+      const double sul = sl[2] + hdt * ftot, sur = sr[2] + hdt * ftot;
+      if (EOS == 0) {
+        double t1 = 0.5 * (sqrt(spl / srl) + sqrt(spr / srr));
+        double t2 = -0.5 * (sur - sul) / t1;
+        double pm = sqrt(spl * spr) * exp(t2);
+        S.umid[n] = sul - t1 * log(pm / spl);
+        S.pmid[n] = fmax(kSmallp, pm);
+      } else {
+        double um, pm;
+        riemann_isentropic(spl, srl, sul, spr, srr, sur, ph, um, pm);
+        S.umid[n] = um;
+        S.pmid[n] = pm;
+      }
     }
   }
   __syncthreads();
 
   // ---- evolve evolve.cu:3-166 (vfac = tmp1) ----
+  // vfac is read only where this chunk sets it below (xa0 + delx, then the
+  // geometry factor), so the reference's first fill of it is not needed
   double *vfac = S.tmp1;
   const double xa0n = S.xa0[n];
   double xa = xa0n, dvol = c.dvol0, dtdm = 0.0, fto1 = 0.0, fto2 = 0.0;
-  if (act) vfac[n] = S.xa0[n] + 0.5 * S.dx0[n];
-  __syncthreads();
   if (n >= 3 && n < nmax - 2) {
     double delx;
     if (AXIS == 0) delx = dt * S.umid[n];
@@ -227,7 +234,7 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
     S.dx[n] = vfac[n + 1] - vfac[n];
     xa = vfac[n];
   }
-  __syncthreads();
+  // the centre forces read this cell's own new width only: no barrier
   // polar sweep: sin of the new centre angle, reused by the volume below
   double sxcl = 0.0;
   if (n >= 3 && n < nmax - 3) {
@@ -285,9 +292,15 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   }
   __syncthreads();
 
-  // ---- remap remap.cu:14-226: al = tmp1, da = umid, a6 = pmid, flux = dx ----
-  al = S.tmp1; da = S.umid; a6 = S.pmid;
-  paraset(n, 3, nmax - 3, par, S.dx, al, da, a6);
+  // ---- remap remap.cu:14-226 ----
+  // paraset on the Lagrangian widths (temporaries in tmp1/umid/pmid), then
+  // the parabolas of rho and of the momentum-like fields (get_flux
+  // remap.cu:1-10) side by side: al/da/a6 in p/q/dx0 (rho), umid/pmid/tmp1
+  // (u), s0/s1/s2 (v or w) and s3/s4/s5 (w in 3D).  The fluxes, each the
+  // reference's expression, go to the al arrays once every cell has read its
+  // neighbour's parabola.  2D slots that stay exactly zero are skipped: w in
+  // the radial sweep, v (= w) in the azimuthal one, whose w slot carries v_r.
+  paraset(n, 3, nmax - 3, par, S.dx, S.tmp1, S.umid, S.pmid);
   double lvol = 0.0;
   if (AXIS == 0) {
     if (!SPH) { lvol = xa - xa0n; lvol *= (xa0n + 0.5 * lvol); }
@@ -302,50 +315,54 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   }
   double dxf = xa - xa0n;
   const bool delC = (dxf >= 0.0);
-  parabola(n, 3, nmax - 3, flat, S.r, al, da, a6, par);
-  double *flux = S.dx;
   double dxnn = 0.0, dxnm = 0.0;
   if (n >= 6 && n < nmax - 5) { dxnn = S.dx[n]; dxnm = S.dx[n - 1]; }
-  __syncthreads();
-  double dxf2 = 0.0, fr = 0.0;
+  constexpr int NF = (THREED ? 4 : 3);
+  double *fld[NF];
+  fld[0] = S.r;
+  fld[1] = S.u;
+  if (THREED) { fld[2] = S.v; fld[NF - 1] = S.w; }
+  else fld[2] = (AXIS == 1) ? S.w : S.v;
+  double *const al[4] = {S.p, S.umid, S.s0, S.s3};
+  double *const da[4] = {S.q, S.pmid, S.s1, S.s4};
+  double *const a6[4] = {S.dx0, S.tmp1, S.s2, S.s5};
+  parabola_n<NF>(n, 3, nmax - 3, flat, fld, al, da, a6, par);
+  double fx[NF];
+  double dxf2 = 0.0;
   if (n >= 6 && n < nmax - 5) {
     if (delC) {
       dxf = 0.5 * dxf / dxnm;
       dxf2 = 1.0 - kFourthd * dxf;
-      fr = (al[n - 1] + da[n - 1] - dxf * (da[n - 1] - dxf2 * a6[n - 1])) * lvol;
     } else {
       dxf = 0.5 * dxf / dxnn;
       dxf2 = 1.0 + kFourthd * dxf;
-      fr = (al[n] - dxf * (da[n] + dxf2 * a6[n])) * lvol;
     }
-    flux[n] = fr;
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      double t;
+      if (delC) t = al[f][n - 1] + da[f][n - 1] - dxf * (da[f][n - 1] - dxf2 * a6[f][n - 1]);
+      else      t = al[f][n] - dxf * (da[f][n] + dxf2 * a6[f][n]);
+      fx[f] = t * (f == 0 ? lvol : fx[0]);
+    }
   }
   __syncthreads();
-  double mm = 0.0, invm = 0.0;
-  if (n >= 6 && n < nmax - 6) {
-    mm = S.r[n] * dvol;
-    double lv = (mm + fr - flux[n + 1]) / c.dvol0;
-    S.r[n] = fmax(kSmallr, lv);
-    invm = 1.0 / (S.r[n] * c.dvol0);
+  if (n >= 6 && n < nmax - 5) {
+#pragma unroll
+    for (int f = 0; f < NF; f++) al[f][n] = fx[f];
   }
-  // momentum-like remaps (get_flux remap.cu:1-10)
-  auto remap_field = [&](double *fld) {
-    parabola(n, 3, nmax - 3, flat, fld, al, da, a6, par);
-    if (n >= 6 && n < nmax - 5) {
-      if (delC) flux[n] = (al[n - 1] + da[n - 1] - dxf * (da[n - 1] - dxf2 * a6[n - 1])) * fr;
-      else      flux[n] = (al[n] - dxf * (da[n] + dxf2 * a6[n])) * fr;
+  __syncthreads();
+  if (n >= 6 && n < nmax - 6) {
+    const double fr = fx[0];
+    const double mm = S.r[n] * dvol;
+    double lv = (mm + fr - al[0][n + 1]) / c.dvol0;
+    S.r[n] = fmax(kSmallr, lv);
+    const double invm = 1.0 / (S.r[n] * c.dvol0);
+#pragma unroll
+    for (int f = 1; f < NF; f++) {
+      double fl = fx[f] - al[f][n + 1];
+      fld[f][n] = (fld[f][n] * mm + fl) * invm;
     }
-    __syncthreads();
-    if (n >= 6 && n < nmax - 6) {
-      double fl = flux[n] - flux[n + 1];
-      fld[n] = (fld[n] * mm + fl) * invm;
-    }
-  };
-  // 2D slots that stay exactly zero are skipped: w in the radial sweep,
-  // v (= w) in the azimuthal one, whose w slot carries v_r
-  remap_field(S.u);
-  if (AXIS != 1 || THREED) remap_field(S.v);
-  if (AXIS == 1 || THREED) remap_field(S.w);
+  }
   __syncthreads();
 }
 

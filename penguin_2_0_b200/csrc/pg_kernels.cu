@@ -75,7 +75,7 @@ __device__ __forceinline__ bool load_step(const SweepCtl &c, StepIn &s) {
 // One radial pencil chunk: column j0, chunk l, polar layer k.  The body is
 // shared by the per-run kernel and the batched kernels of pg_batch.cu.
 template <bool SPH, bool THREED, int NT, int EOS = 0>
-__device__ __forceinline__ void sweep_x_body(ChunkShmT<NT> &S, int n, bool store, const Tables &T, const Planes &P,
+__device__ __forceinline__ void sweep_x_body(ChunkShmData<NT> &S, int n, bool store, const Tables &T, const Planes &P,
                                              const Phys &ph, const SweepCtl &ctl, const StepIn &st, int j0, int l,
                                              int k) {
   const bool last = (l == T.cx.loop - 1);
@@ -191,6 +191,30 @@ __global__ void __launch_bounds__(4 * PX_LIM, MINB) k_sweep_x_packed(Tables T, P
   const bool store = col < npen;
   if (!store) col = npen - 1;
   sweep_x_body<SPH, THREED, PX_LIM>(S[p], n, store, T, P, ph, ctl, st, col % T.nphi, T.cx.loop - 1, col / T.nphi);
+}
+
+// Full radial chunks of PACK adjacent columns per CTA (128 * PACK threads,
+// thread t on cell t / PACK of column t % PACK): a warp's loads and stores of
+// one ring cover PACK adjacent doubles, where one column per CTA touches a
+// separate 32-byte sector per cell.  Columns past the last one repeat it
+// without storing.  The pencils' shared blocks are dynamic (4 of them exceed
+// the 48 KiB a kernel may declare statically) and padded to 128 / PACK mod
+// 128 bytes, so the pencils' accesses fall in different banks.
+template <int PACK>
+using PxShm = ChunkShmT<ARR, 128 / PACK>;
+template <int PACK>
+constexpr int px_shm_bytes() { return PACK * (int)sizeof(PxShm<PACK>); }
+template <bool SPH, bool THREED, int PACK, int MINB>
+__global__ void __launch_bounds__(ARR * PACK, MINB) k_sweep_x_cols(Tables T, Planes P, Phys ph, SweepCtl ctl) {
+  extern __shared__ __align__(16) unsigned char px_shm[];
+  PxShm<PACK> *S = reinterpret_cast<PxShm<PACK> *>(px_shm);
+  StepIn st;
+  if (!load_step(ctl, st)) return;
+  const int p = threadIdx.x % PACK, n = threadIdx.x / PACK;
+  int col = blockIdx.x * PACK + p;
+  const bool store = col < T.nphi;
+  if (!store) col = T.nphi - 1;
+  sweep_x_body<SPH, THREED, ARR>(S[p], n, store, T, P, ph, ctl, st, col, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -448,7 +472,7 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmData<NT> &S, int n, bool st
     S.w[n] = v * rad_cyl;       // angular momentum about the axis
   }
   __syncthreads();
-  ppm_chunk<2, true, true, EOS>(S, n, lim, st.dt, st.frrot, c, st.pl, ph);
+  ppm_chunk<2, true, true, EOS>(S, n, lim, st.dt, st.frrot, c, st.pl, ph, T.zpar + 5 * REAL * l);
   if (ph.visc) {
     double rho = 0.0, nr = 0.0, ddu = 0.0, ddv = 0.0;
     if (act) {
@@ -542,9 +566,16 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_z(Tables T, Planes P, Phys p
 // the last column repeat the last one without storing.
 constexpr int PZ_LIM = 56;
 constexpr int PZ8_THREADS = 352;   // 8 pencils of up to 44 cells, 3 CTAs per SM
+template <int PACK>
+using PzShm = ChunkShmT<PZ_LIM, 128 / PACK>;
+template <int PACK>
+constexpr int pz_shm_bytes() { return PACK * (int)sizeof(PzShm<PACK>); }
 template <int PACK, int MINB, int MAXT = PACK * PZ_LIM>
 __global__ void __launch_bounds__(MAXT, MINB) k_sweep_z_packed(Tables T, Planes P, Phys ph, SweepCtl ctl, int ntop) {
-  __shared__ ChunkShmT<PZ_LIM, 128 / PACK> S[PACK];
+  // the PACK pencils' shared blocks, dynamic: 8 of them (67 KB) exceed the
+  // 48 KiB a kernel may declare statically
+  extern __shared__ __align__(16) unsigned char pz_shm[];
+  PzShm<PACK> *S = reinterpret_cast<PzShm<PACK> *>(pz_shm);
   StepIn st;
   if (!load_step(ctl, st)) return;
   const int p = threadIdx.x % PACK, n = threadIdx.x / PACK;
@@ -563,12 +594,20 @@ __global__ void k_tables(Tables T, Phys ph, int ndim, double kill_rin, double ki
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int n = T.nk * T.nrg;
   if (t >= n) return;
-  if (t < T.nk + 2 * NPAD) {
+  const int nz = T.nk + 2 * NPAD;
+  if (t < nz) {
     // sin, cos of every polar layer's centre angle (ghost layers included)
     const_cast<double *>(T.szc)[t] = sin(T.zc[t]);
     const_cast<double *>(T.czc)[t] = cos(T.zc[t]);
     const_cast<double *>(T.szf)[t] = sin(T.z[t]);
     const_cast<double *>(T.czf)[t] = cos(T.z[t]);
+    // the polar sweep's Eulerian paraset coefficients: every polar pencil
+    // has the layers' widths dz, so they are one set per layer (c0..c2 where
+    // dz[t + 2] exists, c3 and c4 where dz[t + 1] does)
+    Par par{0.0, 0.0, 0.0, 0.0, 0.0};
+    if (t >= 1 && t + 1 < nz) paraset_at(T.dz, t, t + 2 < nz, par);
+    double *zp = const_cast<double *>(T.zpar) + 5 * t;
+    zp[0] = par.c0; zp[1] = par.c1; zp[2] = par.c2; zp[3] = par.c3; zp[4] = par.c4;
   }
   int k = t / T.nrg, row = t % T.nrg;
   double rad = T.rxc[row];
@@ -1354,9 +1393,27 @@ static void sweep_x_t(const Tables &T, const Planes &P, const Phys &ph, const Sw
   const int occ8 = T.occ8;
   int full = ch.stuck ? ch.loop : ch.loop - 1;
   if (full > 0) {
-    dim3 grid(T.nphi, full, T.nk);
-    if (ndim == 3) launch_x<true, true, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
-    else launch_x<false, false, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
+    bool done = false;
+    if constexpr (EOS == 0) {
+      // a stuck last chunk (imax % 116 == 0) keeps the one-column kernel
+      const int xp = (ch.stuck || !occ8) ? 1 : T.xpack;
+      if (xp == 2 || xp == 4) {
+        dim3 grid((T.nphi + xp - 1) / xp, ch.loop - 1, T.nk);
+        if (xp == 2) {
+          if (ndim == 3) k_sweep_x_cols<true, true, 2, 4><<<grid, 2 * ARR, px_shm_bytes<2>(), s>>>(T, P, ph, c);
+          else k_sweep_x_cols<false, false, 2, 4><<<grid, 2 * ARR, px_shm_bytes<2>(), s>>>(T, P, ph, c);
+        } else {
+          if (ndim == 3) k_sweep_x_cols<true, true, 4, 2><<<grid, 4 * ARR, px_shm_bytes<4>(), s>>>(T, P, ph, c);
+          else k_sweep_x_cols<false, false, 4, 2><<<grid, 4 * ARR, px_shm_bytes<4>(), s>>>(T, P, ph, c);
+        }
+        done = true;
+      }
+    }
+    if (!done) {
+      dim3 grid(T.nphi, full, T.nk);
+      if (ndim == 3) launch_x<true, true, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
+      else launch_x<false, false, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
+    }
   }
   if (!ch.stuck) {
     if constexpr (EOS == 0) {
@@ -1409,9 +1466,10 @@ static void sweep_z_t(const Tables &T, const Planes &P, const Phys &ph, const Sw
     if (T.zpack && ch.loop == 1 && !ch.stuck && ch.lim_last <= PZ_LIM) {
       int npen = T.nr * T.nphi;
       if (8 * ch.lim_last <= PZ8_THREADS)    // whole warps: 8 pencils of 44 cells (kmax 32) are 11
-        k_sweep_z_packed<8, 3, PZ8_THREADS><<<(npen + 7) / 8, 8 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
+        k_sweep_z_packed<8, 3, PZ8_THREADS><<<(npen + 7) / 8, 8 * ch.lim_last, pz_shm_bytes<8>(), s>>>(T, P, ph, c,
+                                                                                                        ntop);
       else
-        k_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
+        k_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, pz_shm_bytes<4>(), s>>>(T, P, ph, c, ntop);
       return;
     }
   }
@@ -1432,6 +1490,33 @@ void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c
 
 // kernels launched by one sweep_* call
 int sweep_launches(const Chunking &ch) { return (ch.stuck || ch.loop == 1) ? 1 : 2; }
+
+// Per-device kernel attributes, set with the device current before the first
+// launch (pg_create): the packed polar kernels take their shared blocks as
+// dynamic shared memory, above the 48 KiB default limit for the 8-pencil
+// form, and prefer the largest shared-memory carveout so that 3 CTAs of it
+// (201 KB) fit on an SM.
+int setup_device() {
+  cudaError_t e = cudaFuncSetAttribute(k_sweep_z_packed<8, 3, PZ8_THREADS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, pz_shm_bytes<8>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sweep_z_packed<8, 3, PZ8_THREADS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             100);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sweep_z_packed<4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             pz_shm_bytes<4>());
+  // the column-packed radial kernels: 2 columns (37 KB) or 4 (75 KB) per CTA
+  const void *cols2[2] = {(const void *)k_sweep_x_cols<true, true, 2, 4>, (const void *)k_sweep_x_cols<false, false, 2, 4>};
+  const void *cols4[2] = {(const void *)k_sweep_x_cols<true, true, 4, 2>, (const void *)k_sweep_x_cols<false, false, 4, 2>};
+  for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+    e = cudaFuncSetAttribute(cols2[i], cudaFuncAttributeMaxDynamicSharedMemorySize, px_shm_bytes<2>());
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(cols4[i], cudaFuncAttributeMaxDynamicSharedMemorySize, px_shm_bytes<4>());
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(cols4[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  }
+  return e == cudaSuccess ? 0 : 1;
+}
 
 void cfl_full(const Tables &T, const double *r, const double *u, const double *v, const double *w,
               const double *p0, const Phys &ph, double frrot, int ndim, unsigned long long *out,

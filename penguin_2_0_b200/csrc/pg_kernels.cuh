@@ -29,6 +29,7 @@ struct Tables {
   int nr, nphi, nk, nrg;
   int occ8;                                     // 128-thread sweeps capped at 64 registers (8 CTAs/SM)
   int zpack;                                    // polar pencils per CTA when nk is one chunk (0: one per CTA)
+  int xpack;                                    // radial columns per CTA of the full chunks (1, 2 or 4)
   Chunking cx, cy, cz;
   const double *rx, *rdx, *rxvol, *rxc;         // [nrg]
   const double *radc, *cs2, *nu;                // [nk*nrg]
@@ -37,6 +38,7 @@ struct Tables {
   const double *z, *dz, *zvol, *zc;             // [nk + 12]: 6 ghost layers each side
   const double *szc, *czc;                      // [nk + 12]: sin(zc), cos(zc) (k_tables)
   const double *szf, *czf;                      // [nk + 12]: sin(z), cos(z) of the layer faces
+  const double *zpar;                           // [5 (nk + 12)]: Eulerian paraset c0..c4 per layer (k_tables)
   const double *val_r, *val_u, *val_v;          // [nk*nrg] damping / FARGO targets
   const double *damp_g, *damp_pw;               // [nk*nrg] zone factor, r^-1.5
   const double *tg;                             // [6*nr*4] theta ghost state (udr): r,p,u,v
@@ -127,6 +129,8 @@ void sweep_x(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c
 void sweep_y(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s);
 void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s);
 int sweep_launches(const Chunking &ch);
+// per-device kernel attributes (dynamic shared memory limits); 0 on success
+int setup_device();
 void cfl_full(const Tables &T, const double *r, const double *u, const double *v, const double *w,
               const double *p0, const Phys &ph, double frrot, int ndim, unsigned long long *out,
               cudaStream_t s);

@@ -97,12 +97,15 @@ struct Par { double c0, c1, c2, c3, c4; };
 
 // Shared arrays of one chunk: the sweep kernel's (ppm.cu:38-39) and
 // ppmlr's (ppmlr.cu:7-10).  q only serves as parabola storage (al) because
-// the q remap is dead in EOS 0 and 1.  NT is the CTA size: 128 for full
-// chunks, 64 or 32 for a short last chunk (lim <= NT).
+// the q remap is dead in EOS 0 and 1.  s0..s5 are scratch of the parabolas
+// that run side by side (three in states, up to four in remap), where the
+// reference runs them one after another through q/dx/tmp1.  NT is the CTA
+// size: 128 for full chunks, 64 or 32 for a short last chunk (lim <= NT).
 template <int NT>
 struct ChunkShmData {
   double r[NT + 2], p[NT + 2], u[NT + 2], v[NT + 2], w[NT + 2], xa0[NT + 2], dx0[NT + 2];
   double q[NT + 2], dx[NT + 2], umid[NT + 2], pmid[NT + 2], tmp1[NT + 2];
+  double s0[NT + 2], s1[NT + 2], s2[NT + 2], s3[NT + 2], s4[NT + 2], s5[NT + 2];
   // cos(phi - phi_planet) at the start of the step: one value for a radial
   // or polar pencil, whose cells share the azimuth phi (written by cell 0)
   double cf0;
@@ -258,6 +261,35 @@ __device__ __forceinline__ void paraset(int n, int nmin, int nmax, Par &par, con
   __syncthreads();
 }
 
+// paraset's coefficients at index L of a width array (the same arithmetic as
+// paraset for a cell n = L inside the chunk): c0..c2 need dx[L-1..L+2], c3,
+// c4 dx[L-1..L+1].  Used to tabulate the polar sweep's Eulerian
+// coefficients once per layer, since every polar pencil has the same widths.
+__device__ __forceinline__ void paraset_at(const double *dx, int L, bool full, Par &par) {
+  const double dx_n = dx[L];
+  const double an = dx_n + dx[L + 1];
+  const double ain = 1.0 / an;
+  const double bn = an + dx_n;
+  const double bi = 1.0 / bn;
+  const double c = an + dx[L + 1];
+  const double ci = 1.0 / c;
+  const double am = dx[L - 1] + dx_n;          // a[n-1]
+  const double aim = 1.0 / am;                 // ai[n-1]
+  const double bm = am + dx[L - 1];            // b[n-1]
+  if (full) {
+    const double ap = dx[L + 1] + dx[L + 2];   // a[n+1]
+    double d = 1.0 / (am + ap);
+    par.c0 = dx_n * ain * (1.0 + 2.0 * d * dx[L + 1] * (am * bi - ap * ci));
+    par.c1 = -d * dx_n * am * bi;
+    par.c2 = d * dx[L + 1] * ap * ci;
+  } else {
+    par.c0 = par.c1 = par.c2 = 0.0;
+  }
+  double d = dx_n / (am + dx[L + 1]);
+  par.c3 = d * bm * ain;
+  par.c4 = d * c * aim;
+}
+
 // parabola parabola.cu:70-133 (CW84 eq 1.5-1.8, 1.10)
 __device__ __forceinline__ void parabola(int n, int nmin, int nmax, double flat, const double *val,
                                          double *al, double *da, double *a6, const Par &par) {
@@ -292,6 +324,63 @@ __device__ __forceinline__ void parabola(int n, int nmin, int nmax, double flat,
     da[n] = xr - la;
     a6[n] = 6.0 * (a - 0.5 * (xr + la));
     al[n] = la;
+  }
+  __syncthreads();
+}
+
+// parabola for NF fields at once: the same three phases and, per field, the
+// same arithmetic as parabola(), with one barrier per phase for all fields
+// instead of one per phase and field.  A field's values and its own a6 are
+// reloaded from shared memory after a barrier (same bits) so that only ar
+// stays in a register across one.
+template <int NF>
+__device__ __forceinline__ void parabola_n(int n, int nmin, int nmax, double flat, const double *const *val,
+                                           double *const *al, double *const *da, double *const *a6,
+                                           const Par &par) {
+  if (n >= nmin + 1 && n < nmax - 1) {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const double a = val[f][n];
+      const double da_r = val[f][n + 1] - a;
+      const double da_l = a - val[f][n - 1];
+      double t1 = par.c3 * da_r + par.c4 * da_l;
+      if (t1 < 0.0) t1 = -min3(-t1, 2.0 * fabs(da_l), 2.0 * fabs(da_r));
+      else          t1 = min3(t1, 2.0 * fabs(da_l), 2.0 * fabs(da_r));
+      if (da_l * da_r < 0.0) t1 = 0.0;
+      a6[f][n] = t1;
+    }
+  }
+  __syncthreads();
+  double ar[NF];
+  if (n >= nmin + 1 && n < nmax - 2) {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const double a = val[f][n];
+      const double da_r = val[f][n + 1] - a;
+      const double t1 = a6[f][n];
+      ar[f] = a + par.c0 * da_r + par.c1 * a6[f][n + 1] + par.c2 * t1;
+      al[f][n + 1] = ar[f];
+    }
+  }
+  __syncthreads();
+  if (n >= nmin + 2 && n < nmax - 2) {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const double a = val[f][n];
+      double u1 = flat * a;
+      double u2 = 1.0 - flat;
+      double xr = u1 + u2 * ar[f];
+      double la = u1 + u2 * al[f][n];
+      u1 = xr - la;
+      u2 = u1 * u1;
+      u1 = u1 * (6.0 * (a - 0.5 * (xr + la)));
+      if ((xr - a) * (a - la) <= 0.0) { xr = a; la = a; }
+      if (u2 < u1) la = 3.0 * a - 2.0 * xr;
+      if (u2 < -u1) xr = 3.0 * a - 2.0 * la;
+      da[f][n] = xr - la;
+      a6[f][n] = 6.0 * (a - 0.5 * (xr + la));
+      al[f][n] = la;
+    }
   }
   __syncthreads();
 }

@@ -172,6 +172,7 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
     return code;
   };
   if (cudaSetDevice(device) != cudaSuccess) { delete run; return PG_ERR_CUDA; }
+  if (pgk::setup_device() != 0) return bail(PG_ERR_CUDA);
   if (cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PG_ERR_CUDA);
   run->plane_elems = (size_t)run->nk * run->nrg * run->nphi;
   run->fp32 = (p->precision == 1);
@@ -189,7 +190,7 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
   int nrg = run->nrg, nphi = run->nphi, nk = run->nk, nr = run->nr;
   size_t nring = (size_t)nk * nrg;
   size_t nz = (size_t)nk + 2 * NPAD;
-  run->tab_elems = 4 * (size_t)nrg + 10 * nring + 4 * (size_t)nphi + 8 * nz + (size_t)2 * NPAD * nr * 4;
+  run->tab_elems = 4 * (size_t)nrg + 10 * nring + 4 * (size_t)nphi + 13 * nz + (size_t)2 * NPAD * nr * 4;
   if (cudaMalloc(&run->tab, run->tab_elems * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
   if (cudaMalloc(&run->itab, 2 * nring * sizeof(int)) != cudaSuccess) return bail(PG_ERR_NOMEM);
   double *t = run->tab;
@@ -206,6 +207,13 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
     // per CTA); same arithmetic per cell either way
     const char *zp = std::getenv("PG_POLAR_PACK");
     T.zpack = (zp && std::atoi(zp) == 0) ? 0 : 4;
+    // full radial chunks: 2 adjacent azimuth columns per CTA by default
+    // (PG_RADIAL_PACK 1 or 4 for one or four); same arithmetic per cell.
+    // Measured on the 128x1024x32 disk: radial 0.727 ms with one column per
+    // CTA, 0.660 with two, 0.697 with four
+    const char *xp = std::getenv("PG_RADIAL_PACK");
+    T.xpack = xp ? std::atoi(xp) : 2;
+    if (T.xpack != 2 && T.xpack != 4) T.xpack = 1;
   }
   T.cx = pgd::make_chunking(nr);
   T.cy = pgd::make_chunking(nphi);
@@ -219,6 +227,7 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
   T.y = t; t += nphi; T.dy = t; t += nphi; T.yvol = t; t += nphi; T.yc = t; t += nphi;
   T.z = t; t += nz; T.dz = t; t += nz; T.zvol = t; t += nz; T.zc = t; t += nz;
   T.szc = t; t += nz; T.czc = t; t += nz; T.szf = t; t += nz; T.czf = t; t += nz;
+  T.zpar = t; t += 5 * nz;
   T.tg = t; t += (size_t)2 * NPAD * nr * 4;
   if (cudaMalloc(&T.rot_v, nring * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
   if (cudaMalloc(&run->vbg, nring * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
@@ -1171,7 +1180,7 @@ extern "C" size_t pg_run_device_bytes(const pg_params *p) {
   size_t es = (p->precision == 1) ? sizeof(float) : sizeof(double);
   size_t b = 2 * (size_t)nf * up(pe * es);
   if (p->precision != 1) b += up(pe * sizeof(double));                         // p0
-  b += up((4 * nrg + 10 * nring + 4 * nphi + 8 * nz + 2 * NPAD * nr * 4) * sizeof(double));
+  b += up((4 * nrg + 10 * nring + 4 * nphi + 13 * nz + 2 * NPAD * nr * 4) * sizeof(double));
   b += up(2 * nring * sizeof(int)) + 3 * up(nring * sizeof(double));           // itab, rot_v, vbg, sbg
   b += up(nr * nk * sizeof(double)) + up(4) + up(32) + up(8) + up(sizeof(pgd::DevClock));
   b += up((size_t)4096 * pgd::HIST_COLS * sizeof(double));

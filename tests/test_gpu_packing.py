@@ -38,3 +38,33 @@ def test_packed_short_chunks_are_bitwise(gpu, monkeypatch, case):
             out[pack] = pg.dump_fields(r.save(), p)
     for k in ("r", "u", "v", "w", "rot_j"):
         np.testing.assert_array_equal(out["4"][k], out["0"][k], err_msg=k)
+
+
+RADIAL_CASES = [
+    dict(which=0, imax=256, jmax=384),                        # 2 full radial chunks per column + packed last chunk
+    dict(which=0, imax=252, jmax=390),                        # jmax not a multiple of 4: padding columns
+    dict(which=1, imax=128, jmax=132, kmax=16),               # 3D
+    dict(which=0, imax=232, jmax=200),                        # imax % 116 == 0: stuck last chunk
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", RADIAL_CASES)
+def test_radial_column_packing_is_bitwise(gpu, monkeypatch, case):
+    """Full radial chunks run one column per CTA, or 2 or 4 adjacent columns
+    per CTA (PG_RADIAL_PACK): the same device body per cell, so the results
+    must be bitwise equal."""
+    c = dict(case)
+    p = pg.params(c.pop("which"), nprin=1, **c)
+    ic = pg.build_ic(p)
+    out = {}
+    for pack in ("1", "2", "4"):
+        monkeypatch.setenv("PG_RADIAL_PACK", pack)
+        with pg.Run(p, 0) as r:
+            r.load(ic)
+            r.clock_reset(0)
+            r.advance(4)
+            out[pack] = pg.dump_fields(r.save(), p)
+    for pack in ("2", "4"):
+        for k in ("r", "u", "v", "w", "rot_j"):
+            np.testing.assert_array_equal(out[pack][k], out["1"][k], err_msg=f"{k} pack {pack}")

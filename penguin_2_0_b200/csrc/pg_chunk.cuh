@@ -57,10 +57,16 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
     else ftot = ph.plnt ? grav_azi_sph_s(c.rad, azi, c.sinpol, pl, hdt) : 0.0;
   } else {
     // get_fz_bound forces.cu:298-334 (ngeomz 5) at the face angle xa0[n],
-    // whose sin and cos come from the per-layer table
-    double azi = c.azi + hdt * c.vrot;
+    // whose sin and cos come from the per-layer table; the planet's angle
+    // factor cos(azi + hdt v_rot - (p.y + hdt p.vy)) by angle addition from
+    // the pencil's start-of-step cos and sin of azi - p.y
     const double sp = c.sinfz, cp = c.cosfz;
-    double grav = ph.plnt ? grav_pol_sph_s(c.rad, azi, sp, cp, pl, hdt) : 0.0;
+    double grav = 0.0;
+    if (ph.plnt) {
+      double sd, cd;
+      sincos_small(hdt * (c.vrot - pl.vy), sd, cd);
+      grav = grav_pol_sph_cf(c.rad, S.cf0 * cd - S.sf0 * sd, sp, cp, pl);
+    }
     double irc = 1.0 / (c.rad * sp);
     double f = grav;
     f += __dmul_rn(sq(0.5 * (S.w[n] + S.w[n - 1])) * cp, __dmul_rn(__dmul_rn(irc, irc), irc));
@@ -247,8 +253,15 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
       fto2 = centre_force<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, c.sinpol, S, pl, ph);
     } else {
       fto1 = centre_force<2, SPH, true>(n, 0.0, c.rad, c.azi, c.pol, 0.0, S, pl, ph, S.cf0, c.sinpol, c.cospol);
-      sxcl = sin(xcl);
-      fto2 = centre_force<2, SPH>(n, dt, c.rad, c.azi + dt * c.vrot, xcl, 0.0, S, pl, ph, 0.0, sxcl, cos(xcl));
+      // sin, cos of the new centre angle from the layer's (xcl moved by a
+      // fraction of a cell), and the planet's angle factor at t + dt from
+      // the pencil's, by angle addition
+      double se, ce, sd, cd;
+      sincos_small(xcl - c.pol, se, ce);
+      sxcl = c.sinpol * ce + c.cospol * se;
+      const double cxcl = c.cospol * ce - c.sinpol * se;
+      sincos_small(dt * (c.vrot - pl.vy), sd, cd);
+      fto2 = centre_force<2, SPH, true>(n, dt, c.rad, 0.0, xcl, 0.0, S, pl, ph, S.cf0 * cd - S.sf0 * sd, sxcl, cxcl);
     }
   }
   __syncthreads();
@@ -270,13 +283,19 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
       // evolve.cu:117-124 with cos(a) - cos(b) written as
       // 2 sin((a+b)/2) sin((b-a)/2): the same value without the
       // cancellation that makes the reference's form depend on libm ulps
+      // Sines of angles a fraction of a cell from the face angle xa0 come
+      // from its per-layer sin and cos by angle addition (sincos_small).
       double delx = xa - xa0n;
-      const double sc = (n < nmax - 3) ? sxcl : sin(xa + 0.5 * dxn);
-      dvol = 2.0 * sc * sin(0.5 * dxn) * c.rad;
-      if (delx == 0.0) vfac[n] = sin(xa);
+      double sw, cw;
+      sincos_small(0.5 * dxn, sw, cw);
+      const double sc = (n < nmax - 3) ? sxcl : c.sinfz * cw + c.cosfz * sw;   // sin(xa0 + dxn / 2)
+      dvol = 2.0 * sc * sw * c.rad;
+      if (delx == 0.0) vfac[n] = c.sinfz;                                     // sin(xa) = sin(xa0)
       else {
-        sA = sin(xa0n + 0.5 * delx);
-        sB = sin(0.5 * delx);
+        double sh, ch;
+        sincos_small(0.5 * delx, sh, ch);
+        sA = c.sinfz * ch + c.cosfz * sh;                                        // sin(xa0 + delx / 2)
+        sB = sh;
         haveS = true;
         vfac[n] = 2.0 * sA * sB / delx;
       }
@@ -311,7 +330,11 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
     // remap.cu:53, cancellation-free form of (cos(xa0) - cos(xa)) * rad
     double d = xa - xa0n;
     if (haveS) lvol = 2.0 * sA * sB * c.rad;
-    else lvol = 2.0 * sin(xa0n + 0.5 * d) * sin(0.5 * d) * c.rad;
+    else {
+      double sh, ch;
+      sincos_small(0.5 * d, sh, ch);
+      lvol = 2.0 * (c.sinfz * ch + c.cosfz * sh) * sh * c.rad;
+    }
   }
   double dxf = xa - xa0n;
   const bool delC = (dxf >= 0.0);

@@ -40,6 +40,7 @@ template <int NT>
 struct ChunkShm32Data {
   float r[NT + 2], p[NT + 2], u[NT + 2], v[NT + 2], w[NT + 2], dx0[NT + 2];
   float q[NT + 2], dx[NT + 2], umid[NT + 2], pmid[NT + 2], tmp1[NT + 2], dl[NT + 2];
+  float s0[NT + 2], s1[NT + 2], s2[NT + 2], s3[NT + 2], s4[NT + 2], s5[NT + 2];   // side-by-side parabolas
   double L[NT + 2], Lal[NT + 2], Lda[NT + 2], La6[NT + 2], Lflux[NT + 2], xa0[NT + 2];
   double Rd[NT + 2], dld[NT + 2];   // FP64 Lagrangian density and face displacements
   double cf0;   // cos(phi - phi_planet) at the start of the step (radial, polar pencils)
@@ -140,6 +141,62 @@ __device__ __forceinline__ void parabola32(int n, int nmin, int nmax, float flat
     da[n] = xr - la;
     a6[n] = six * (a - half * (xr + la));
     al[n] = la;
+  }
+  __syncthreads();
+}
+
+// parabola32 for NF float fields at once: the same phases and, per field,
+// the same arithmetic, one barrier per phase for all fields (see
+// parabola_n); a field's value and its own a6 are reloaded after a barrier
+template <int NF>
+__device__ __forceinline__ void parabola32_n(int n, int nmin, int nmax, float flat, const float *const *val,
+                                             float *const *al, float *const *da, float *const *a6,
+                                             const ParF &par) {
+  if (n >= nmin + 1 && n < nmax - 1) {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const float a = val[f][n];
+      const float da_r = val[f][n + 1] - a;
+      const float da_l = a - val[f][n - 1];
+      float t1 = par.c3 * da_r + par.c4 * da_l;
+      const float m1 = 2.0f * fabsf(da_l), m2 = 2.0f * fabsf(da_r);
+      if (t1 < 0) { float x = -t1; float mn = (x < m1) ? ((m2 < x) ? m2 : x) : ((m2 < m1) ? m2 : m1); t1 = -mn; }
+      else        { float x = t1;  float mn = (x < m1) ? ((m2 < x) ? m2 : x) : ((m2 < m1) ? m2 : m1); t1 = mn; }
+      if (da_l * da_r < 0) t1 = 0;
+      a6[f][n] = t1;
+    }
+  }
+  __syncthreads();
+  float ar[NF];
+  if (n >= nmin + 1 && n < nmax - 2) {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const float a = val[f][n];
+      const float da_r = val[f][n + 1] - a;
+      const float t1 = a6[f][n];
+      ar[f] = a + par.c0 * da_r + par.c1 * a6[f][n + 1] + par.c2 * t1;
+      al[f][n + 1] = ar[f];
+    }
+  }
+  __syncthreads();
+  if (n >= nmin + 2 && n < nmax - 2) {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const float a = val[f][n];
+      float u1 = flat * a;
+      float u2 = 1.0f - flat;
+      float xr = u1 + u2 * ar[f];
+      float la = u1 + u2 * al[f][n];
+      u1 = xr - la;
+      u2 = u1 * u1;
+      u1 = u1 * (6.0f * (a - 0.5f * (xr + la)));
+      if ((xr - a) * (a - la) <= 0) { xr = a; la = a; }
+      if (u2 < u1) la = 3.0f * a - 2.0f * xr;
+      if (u2 < -u1) xr = 3.0f * a - 2.0f * la;
+      da[f][n] = xr - la;
+      a6[f][n] = 6.0f * (a - 0.5f * (xr + la));
+      al[f][n] = la;
+    }
   }
   __syncthreads();
 }
@@ -266,31 +323,31 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
     S.umid[n] = cs;
     S.pmid[n] = 1.0f - kFourthdF * cs;
   }
+  // the parabolas of p, rho and u side by side (parabola32_n): al/da/a6 in
+  // q/dx/tmp1 (p), s0/s1/s2 (rho), s3/s4/s5 (u)
   float spl = 0.f, spr = 0.f, srl = 0.f, srr = 0.f, sul = 0.f, sur = 0.f;
   const float *cs = S.umid, *csfac = S.pmid;
   float *al = S.q, *da = S.dx, *a6 = S.tmp1;
-  parabola32<float>(n, 0, nmax, flat, S.p, al, da, a6, par);
-  if (n >= 3 && n < nmax - 2) {
-    float t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
-    spl = fmaxf(kSmallpF, t);
-    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
-    spr = fmaxf(kSmallpF, t);
-  }
-  __syncthreads();
-  parabola32<float>(n, 0, nmax, flat, S.r, al, da, a6, par);
-  if (n >= 3 && n < nmax - 2) {
-    float t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
-    srl = fmaxf(kSmallrF, t);
-    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
-    srr = fmaxf(kSmallrF, t);
-  }
-  __syncthreads();
-  parabola32<float>(n, 0, nmax, flat, S.u, al, da, a6, par);
-  if (n >= 3 && n < nmax - 2) {
-    float t = al[n - 1] + da[n - 1] - cs[n - 1] * (da[n - 1] - csfac[n - 1] * a6[n - 1]);
-    sul = t + hdtf * ftot;
-    t = al[n] + cs[n] * (da[n] + csfac[n] * a6[n]);
-    sur = t + hdtf * ftot;
+  {
+    const float *val[3] = {S.p, S.r, S.u};
+    float *const al3[3] = {S.q, S.s0, S.s3};
+    float *const da3[3] = {S.dx, S.s1, S.s4};
+    float *const a63[3] = {S.tmp1, S.s2, S.s5};
+    parabola32_n<3>(n, 0, nmax, flat, val, al3, da3, a63, par);
+    if (n >= 3 && n < nmax - 2) {
+      float sl[3], sr[3];
+#pragma unroll
+      for (int f = 0; f < 3; f++) {
+        sl[f] = al3[f][n - 1] + da3[f][n - 1] - cs[n - 1] * (da3[f][n - 1] - csfac[n - 1] * a63[f][n - 1]);
+        sr[f] = al3[f][n] + cs[n] * (da3[f][n] + csfac[n] * a63[f][n]);
+      }
+      spl = fmaxf(kSmallpF, sl[0]);
+      spr = fmaxf(kSmallpF, sr[0]);
+      srl = fmaxf(kSmallrF, sl[1]);
+      srr = fmaxf(kSmallrF, sr[1]);
+      sul = sl[2] + hdtf * ftot;
+      sur = sr[2] + hdtf * ftot;
+    }
   }
   __syncthreads();
   // ---- riemann (isothermal) ----
@@ -439,16 +496,40 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
     S.r[n] = (float)sig_new;
     invm = 1.0f / (S.r[n] * (float)c.dvol0);
   }
-  auto remap_f = [&](float *fld) {
-    parabola32<float>(n, 3, nmax - 3, flat, fld, al, da, a6, par);
+  // the FP32 momentum-like fields side by side (parabola32_n): u, plus w in
+  // the radial sweep (3D), w and v in the azimuthal one (v in 3D), v in the
+  // polar one; al/da/a6 in tmp1/umid/pmid, s0/s1/s2, s3/s4/s5; the fluxes go
+  // to the al arrays once every cell has read its neighbour's parabola
+  {
+    constexpr int NF = (AXIS == 0) ? (THREED ? 2 : 1) : (AXIS == 1 ? (THREED ? 3 : 2) : 2);
+    float *fl[3] = {S.u, S.u, S.u};
+    if (AXIS == 0) { fl[1] = S.w; }
+    else if (AXIS == 1) { fl[1] = S.w; fl[2] = S.v; }
+    else { fl[1] = S.v; }
+    float *const al3[3] = {S.tmp1, S.s0, S.s3};
+    float *const da3[3] = {S.umid, S.s1, S.s4};
+    float *const a63[3] = {S.pmid, S.s2, S.s5};
+    parabola32_n<NF>(n, 3, nmax - 3, flat, fl, al3, da3, a63, par);
+    float fx[NF];
     if (n >= 6 && n < nmax - 5) {
-      if (delC) flux[n] = (al[n - 1] + da[n - 1] - dxf * (da[n - 1] - dxf2 * a6[n - 1])) * fr;
-      else      flux[n] = (al[n] - dxf * (da[n] + dxf2 * a6[n])) * fr;
+#pragma unroll
+      for (int f = 0; f < NF; f++) {
+        if (delC) fx[f] = (al3[f][n - 1] + da3[f][n - 1] - dxf * (da3[f][n - 1] - dxf2 * a63[f][n - 1])) * fr;
+        else      fx[f] = (al3[f][n] - dxf * (da3[f][n] + dxf2 * a63[f][n])) * fr;
+      }
     }
     __syncthreads();
-    if (n >= 6 && n < nmax - 6) fld[n] = (fld[n] * mm + (flux[n] - flux[n + 1])) * invm;
-  };
-  remap_f(S.u);
+    if (n >= 6 && n < nmax - 5) {
+#pragma unroll
+      for (int f = 0; f < NF; f++) al3[f][n] = fx[f];
+    }
+    __syncthreads();
+    if (n >= 6 && n < nmax - 6) {
+#pragma unroll
+      for (int f = 0; f < NF; f++) fl[f][n] = (fl[f][n] * mm + (fx[f] - al3[f][n + 1])) * invm;
+    }
+  }
+  (void)flux;
   if (hasL) {
     // FP64 angular momentum: L_new = (L m + F_n - F_{n+1}) / (m + f_n - f_{n+1})
     __syncthreads();   // every thread has read the mass flux of face n+1
@@ -461,9 +542,6 @@ __device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax
     if (n >= 6 && n < nmax - 6) S.L[n] = (S.L[n] * m_d + (S.Lflux[n] - S.Lflux[n + 1])) / mnew_d;
     __syncthreads();
   }
-  if (AXIS == 0) { if (THREED) remap_f(S.w); }
-  else if (AXIS == 1) { remap_f(S.w); if (THREED) remap_f(S.v); }
-  else remap_f(S.v);
   __syncthreads();
   return sig_new;
 }

@@ -272,13 +272,18 @@ __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, cons
     P.ro[o] = r; P.uo[o] = u; P.vo[o] = v;
     if (THREED) P.wo[o] = w;
   };
+  // the cell this thread stores, if any: finish() is called once below, so
+  // the fused epilogue appears once in the kernel's code
+  int jo_st = -1;
+  double st_r = 0.0, st_u = 0.0, st_v = 0.0, st_w = 0.0;
   if (last && T.cy.stuck) {
     // ppm.cu:196 gives this chunk lim = 12: its cells keep their values and
     // only move with the ring's rotation
     int j = REAL * l + n;
     if (n < REAL && j < nphi) {
       size_t s = base + j;
-      finish(wrapm(j + inc, nphi), P.r[s], P.u[s], P.v[s], THREED ? P.w[s] : 0.0);
+      jo_st = wrapm(j + inc, nphi);
+      st_r = P.r[s]; st_u = P.u[s]; st_v = P.v[s]; st_w = THREED ? P.w[s] : 0.0;
     }
   } else {
     const int lim = last ? T.cy.lim_last : ARR;
@@ -351,10 +356,11 @@ __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, cons
       }
     }
     if (n >= NPAD && n < lim - NPAD) {
-      int jo = wrapm(j0 + inc, nphi);
-      finish(jo, S.r[n], S.w[n], S.u[n], THREED ? S.v[n] : 0.0);
+      jo_st = wrapm(j0 + inc, nphi);
+      st_r = S.r[n]; st_u = S.w[n]; st_v = S.u[n]; st_w = THREED ? S.v[n] : 0.0;
     }
   }
+  if (jo_st >= 0) finish(jo_st, st_r, st_u, st_v, st_w);
   if (ctl.fuse) {
     __syncthreads();
     double m = block_max(rate, red);
@@ -419,8 +425,12 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmData<NT> &S, int n, bool st
   c.rad = rad;
   c.azi = T.yc[j0];
   c.pol = 0.0; c.vrot = 0.0; c.dvol0 = 1.0; c.sinpol = 0.0; c.cospol = 0.0; c.sinfz = 0.0; c.cosfz = 0.0;
-  // the pencil's planet angle factor at the start of the step, once
-  if (n == 0) S.cf0 = ph.plnt ? planet_cosfac(c.azi, st.pl, 0.0) : 0.0;
+  // the pencil's planet angle factor at the start of the step, and its
+  // sine (the polar chain's angle additions), once
+  if (n == 0) {
+    S.cf0 = ph.plnt ? planet_cosfac(c.azi, st.pl, 0.0) : 0.0;
+    S.sf0 = ph.plnt ? sin(c.azi - (st.pl.y + 0.0 * st.pl.vy)) : 0.0;
+  }
   double rad_cyl = 1.0;
   size_t idx = 0;
   if (act) {
@@ -480,7 +490,8 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmData<NT> &S, int n, bool st
       rho = S.r[n];
       // nu at this layer's r sin(theta): the table for interior layers, the
       // same expression (get_nu disk_profile.cu:149-152) for ghost layers
-      double nu = (kr >= 0 && kr < nk) ? T.nu[kr * nrg + row] : ph.vis_nu * pow(rad_cyl, ph.p_alpha);
+      double nu = (kr >= 0 && kr < nk) ? T.nu[kr * nrg + row]
+                                        : T.nug[(kr < 0 ? kr + NPAD : kr - nk + NPAD) * T.nr + i];
       nr = nu * rho;
       S.dx0[n] = nr;
     }
@@ -593,7 +604,6 @@ __global__ void k_tables(Tables T, Phys ph, int ndim, double kill_rin, double ki
                          double xmin, double xmax) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int n = T.nk * T.nrg;
-  if (t >= n) return;
   const int nz = T.nk + 2 * NPAD;
   if (t < nz) {
     // sin, cos of every polar layer's centre angle (ghost layers included)
@@ -609,6 +619,17 @@ __global__ void k_tables(Tables T, Phys ph, int ndim, double kill_rin, double ki
     double *zp = const_cast<double *>(T.zpar) + 5 * t;
     zp[0] = par.c0; zp[1] = par.c1; zp[2] = par.c2; zp[3] = par.c3; zp[4] = par.c4;
   }
+  if (ndim == 3 && t < 2 * NPAD * T.nr) {
+    // nu at r sin(theta) of the 12 polar ghost layers of ring i (slot g:
+    // layer g - 6 below the grid, or layer nk + g - 6 above it), the
+    // expression the polar viscosity uses for them (get_nu
+    // disk_profile.cu:149-152)
+    const int i = t % T.nr, g = t / T.nr;
+    const int kz = (g < NPAD) ? g : T.nk + g;          // ghost layer + NPAD
+    const double rcg = T.rxc[i + NPAD] * sin(T.zc[kz]);    // T.szc[kz], which this launch writes
+    const_cast<double *>(T.nug)[t] = ph.vis_nu * pow(rcg, ph.p_alpha);
+  }
+  if (t >= n) return;
   int k = t / T.nrg, row = t % T.nrg;
   double rad = T.rxc[row];
   double rc = rad;
@@ -1632,6 +1653,8 @@ void record(DevClock *clk, cudaStream_t s) {
 void tables(const Tables &T, const Phys &ph, int ndim, double kill_rin, double kill_rout, double xmin,
             double xmax, cudaStream_t s) {
   int n = T.nk * T.nrg;
+  if (2 * NPAD * T.nr > n) n = 2 * NPAD * T.nr;         // the polar ghost-layer nu table
+  if (T.nk + 2 * NPAD > n) n = T.nk + 2 * NPAD;
   k_tables<<<(n + 127) / 128, 128, 0, s>>>(T, ph, ndim, kill_rin, kill_rout, xmin, xmax);
 }
 

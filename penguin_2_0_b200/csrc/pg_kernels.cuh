@@ -39,6 +39,7 @@ struct Tables {
   const double *szc, *czc;                      // [nk + 12]: sin(zc), cos(zc) (k_tables)
   const double *szf, *czf;                      // [nk + 12]: sin(z), cos(z) of the layer faces
   const double *zpar;                           // [5 (nk + 12)]: Eulerian paraset c0..c4 per layer (k_tables)
+  const double *nug;                            // [12 nr]: nu of the polar ghost layers (6 below, 6 above) per ring
   const double *val_r, *val_u, *val_v;          // [nk*nrg] damping / FARGO targets
   const double *damp_g, *damp_pw;               // [nk*nrg] zone factor, r^-1.5
   const double *tg;                             // [6*nr*4] theta ghost state (udr): r,p,u,v

@@ -451,7 +451,8 @@ __device__ __forceinline__ void sweep_z32_body(ChunkShm32<NT> &S, int n, bool st
     const float R = (float)rad;
     if (act) {
       rho = S.r[n];
-      double nu = (kr >= 0 && kr < nk) ? T.nu[kr * nrg + row] : ph.vis_nu * pow(rad_cyl, ph.p_alpha);
+      double nu = (kr >= 0 && kr < nk) ? T.nu[kr * nrg + row]
+                                        : T.nug[(kr < 0 ? kr + NPAD : kr - nk + NPAD) * T.nr + i];
       nr = (float)nu * rho;
       nn[n] = nr;
     }

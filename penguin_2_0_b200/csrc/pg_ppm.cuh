@@ -109,6 +109,8 @@ struct ChunkShmData {
   // cos(phi - phi_planet) at the start of the step: one value for a radial
   // or polar pencil, whose cells share the azimuth phi (written by cell 0)
   double cf0;
+  // sin(phi - phi_planet) at the start of the step (polar pencils, cell 0)
+  double sf0;
 };
 
 // Bytes that bring a per-pencil shared block to TO mod 128.  Kernels that
@@ -125,6 +127,21 @@ template <int NT, int TO = 32>
 struct ChunkShmT : ChunkShmData<NT> {
   char pad_[shm_pad_to((int)sizeof(ChunkShmData<NT>), TO)];
 };
+
+// sin and cos of a small angle by their Taylor series (to x^9 and x^8; for
+// |x| <= 0.05 the first omitted terms are below 1e-21 relative), else by
+// sincos.  The polar sweep's angles move by a fraction of a cell per step,
+// so their sines and cosines follow from per-layer or per-pencil values by
+// angle addition with these.
+__device__ __forceinline__ void sincos_small(double x, double &s, double &c) {
+  if (fabs(x) > 0.05) {
+    sincos(x, &s, &c);
+    return;
+  }
+  const double x2 = x * x;
+  s = x * (1.0 + x2 * (-1.0 / 6.0 + x2 * (1.0 / 120.0 + x2 * (-1.0 / 5040.0 + x2 * (1.0 / 362880.0)))));
+  c = 1.0 + x2 * (-0.5 + x2 * (1.0 / 24.0 + x2 * (-1.0 / 720.0 + x2 * (1.0 / 40320.0))));
+}
 
 // ---- star + planet gravity, forces.cu:23-182 (non-barycentric frame) ------
 // The *_cf forms take cosfac = cos(azi - (p.y + dt p.vy)) from the caller

@@ -100,6 +100,10 @@ LONG_CASES = {
 PERF_CASES = {
     "perf_g252x780": (0, dict(imax=252, jmax=780), 200),
     "perf_g1012x3100": (0, dict(imax=1012, jmax=3100), 40),
+    # the 3D spherical disk's physics on the warp-aligned grid nearest
+    # 128x1024x32: the reference's bundle_sweep2D (radial and azimuthal
+    # sweeps of every layer) against the same two sweeps of ours
+    "perf_g3d136x1012x32": (1, dict(imax=136, jmax=1012, kmax=32), 20),
 }
 
 
@@ -156,14 +160,17 @@ def cmd_perf(rawdir):
         os.makedirs(out, exist_ok=True)
         ic = os.path.join(out, "ic.bin")
         assert L.pg_write_ic(C.byref(p), ic.encode()) == 0
+        write_ghost_override(p, ic)
         exe = os.path.join(ROOT, "oracle", "_ref", case, "penguin_ref")
         r = subprocess.run(["timeout", "-k", "10", "300", exe, ic, str(nsteps), out, "0", "nodiag"],
                            capture_output=True, text=True)
         os.remove(ic)
+        if os.path.exists(ic + ".lft"):
+            os.remove(ic + ".lft")
         if r.returncode != 0:
             raise SystemExit(f"{case}: reference exited {r.returncode}: {r.stderr[-400:]}")
         d = json.loads(r.stdout.strip().splitlines()[-1])
-        cells = p.imax * p.jmax
+        cells = p.imax * p.jmax * p.kmax
         d.update(case=case, zone_updates_per_s=cells * d["steps"] / (d["sweep_ms_total"] / 1e3))
         print(json.dumps(d), flush=True)
 

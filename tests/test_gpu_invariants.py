@@ -73,3 +73,29 @@ def test_fargo_on_and_off_agree_to_truncation_error(gpu):
     # measured with the CPU oracle: 1.3e-5 and 4.7e-6
     assert d[128] <= 3e-5 and d[256] <= 1e-5, d
     assert d[128] / d[256] >= 2.0, d              # falls with resolution: truncation error
+
+
+@pytest.mark.gpu
+def test_polar_sweep_keeps_vertical_equilibrium_to_truncation_error(gpu):
+    """The polar sweep has no reference kernel, so besides the restatement it
+    is held to physics: a 3D disk without planet, noise or viscosity starts in
+    vertical equilibrium (the reference's own initial profile, pinned by
+    tests/test_ic_reference.py), and five polar sweeps may move it only by a
+    truncation error that falls fast with the number of layers over the same
+    polar range (the CPU oracle: L1 3.2e-3, 4.7e-4, 4.9e-5 at 8, 16, 32)."""
+    err = {}
+    for kmax in (8, 16, 32):
+        p = pg.params(1, imax=64, jmax=132, kmax=kmax, plnt_flag=0, noise_amp=0.0, visc_flag=0)
+        with pg.Run(p, 0) as run:
+            ic = pg.build_ic(p)
+            run.load(ic)
+            planet = pg.Planet()
+            dt = pg.get_dt(p.endtime, run, 0.0)
+            for _ in range(5):
+                pg.sweep_axis(run, 2, dt, planet, 0.0)
+            f1 = pg.dump_fields(run.save(), p)
+        f0 = pg.dump_fields(ic, p)
+        err[kmax] = float(np.sum(np.abs(f1["r"] - f0["r"])) / np.sum(np.abs(f0["r"])))
+    print(f"\npolar sweeps from equilibrium, L1(rho): {err}")
+    assert err[32] <= 1e-4, err
+    assert err[8] / err[16] >= 4.0 and err[16] / err[32] >= 4.0, err

@@ -86,3 +86,26 @@ def test_oracle_struct_images_match_the_product_binding():
         assert [(n, t) for n, t in mine._fields_] == [(n, t) for n, t in theirs._fields_]
         for n, _ in mine._fields_:
             assert getattr(mine, n).offset == getattr(theirs, n).offset, n
+
+
+def test_oracle_polar_sweep_keeps_vertical_equilibrium_to_truncation_error():
+    """The restatement of the polar sweep (which has no reference kernel)
+    against physics: from the vertically isothermal equilibrium of a 3D disk
+    without planet, noise or viscosity, five polar sweeps move the density by
+    a truncation error that falls by 4x or more per doubling of the layers."""
+    import ctypes as C
+    from oracle.pyoracle import lib as olib
+    from oracle.abi import pg_body
+    err = {}
+    for kmax in (8, 16, 32):
+        p = pg.params(1, imax=64, jmax=132, kmax=kmax, plnt_flag=0, noise_amp=0.0, visc_flag=0)
+        ic = pg.build_ic(p)
+        o = Oracle(p, ic)
+        b = pg_body()
+        dt = o.get_dt(p.endtime, 0.0)
+        for _ in range(5):
+            olib().orc_sweepz(o._h, dt, C.byref(b), 0.0)
+        f1, f0 = pg.dump_fields(o.save(), p), pg.dump_fields(ic, p)
+        err[kmax] = float(np.sum(np.abs(f1["r"] - f0["r"])) / np.sum(np.abs(f0["r"])))
+    assert err[32] <= 1e-4, err
+    assert err[8] / err[16] >= 4.0 and err[16] / err[32] >= 4.0, err

@@ -153,7 +153,8 @@ def cmd_perf(rawdir):
     the harness) on the perf builds; prints one JSON line per case."""
     from penguin_2_0_b200 import _lib
     L = _lib.lib()
-    for case, (_, _, nsteps) in PERF_CASES.items():
+    for case in _cases(PERF_CASES):
+        nsteps = PERF_CASES[case][2]
         p = params_for(case)
         p.nprin = 100
         out = os.path.join(rawdir, case)

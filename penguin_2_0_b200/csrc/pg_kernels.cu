@@ -179,10 +179,13 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_x(Tables T, Planes P, Phys p
 // t % 4 (a warp's loads of one ring cover 4 adjacent doubles), instead of one
 // column per 32/64-thread CTA with idle lanes.  Columns past the last one
 // repeat it without storing.
+// A last chunk of at most 32 cells (the 128-ring disk's is 12 + 12) takes
+// shared blocks sized for 32: 4.9 KB per pencil instead of 9.5, so about
+// twice as many CTAs fit on an SM.
 constexpr int PX_LIM = 64;
-template <bool SPH, bool THREED, int MINB>
-__global__ void __launch_bounds__(4 * PX_LIM, MINB) k_sweep_x_packed(Tables T, Planes P, Phys ph, SweepCtl ctl) {
-  __shared__ ChunkShmT<PX_LIM> S[4];
+template <bool SPH, bool THREED, int MINB, int LIM = PX_LIM>
+__global__ void __launch_bounds__(4 * LIM, MINB) k_sweep_x_packed(Tables T, Planes P, Phys ph, SweepCtl ctl) {
+  __shared__ ChunkShmT<LIM> S[4];
   StepIn st;
   if (!load_step(ctl, st)) return;
   const int p = threadIdx.x & 3, n = threadIdx.x >> 2;
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(4 * PX_LIM, MINB) k_sweep_x_packed(Tables T, P
   int col = blockIdx.x * 4 + p;
   const bool store = col < npen;
   if (!store) col = npen - 1;
-  sweep_x_body<SPH, THREED, PX_LIM>(S[p], n, store, T, P, ph, ctl, st, col % T.nphi, T.cx.loop - 1, col / T.nphi);
+  sweep_x_body<SPH, THREED, LIM>(S[p], n, store, T, P, ph, ctl, st, col % T.nphi, T.cx.loop - 1, col / T.nphi);
 }
 
 // Full radial chunks of PACK adjacent columns per CTA (128 * PACK threads,
@@ -1440,8 +1443,13 @@ static void sweep_x_t(const Tables &T, const Planes &P, const Phys &ph, const Sw
     if constexpr (EOS == 0) {
       if (T.zpack && ch.lim_last <= PX_LIM) {
         int npen = T.nphi * T.nk, blocks = (npen + 3) / 4, nt = 4 * ch.lim_last;
-        if (ndim == 3) k_sweep_x_packed<true, true, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
-        else k_sweep_x_packed<false, false, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
+        if (ch.lim_last <= 32) {
+          if (ndim == 3) k_sweep_x_packed<true, true, 8, 32><<<blocks, nt, 0, s>>>(T, P, ph, c);
+          else k_sweep_x_packed<false, false, 8, 32><<<blocks, nt, 0, s>>>(T, P, ph, c);
+        } else {
+          if (ndim == 3) k_sweep_x_packed<true, true, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
+          else k_sweep_x_packed<false, false, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
+        }
         return;
       }
     }

@@ -441,8 +441,10 @@ def bench_serve(args):
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": f"mixed: f32 planes for {sum(p.precision for p in reqs)} of {n} requests",
         "data": "synthetic seeded request stream (no public dataset)",
-        "config": {"workload": f"serving {n} requests (sample of the 2000-request stream), orbits "
-                               f"{5 * scale:g}-{50 * scale:g} (x{scale:g} of 5-50), 10% 3D",
+        "config": {"workload": (f"serving the 2000-request stream as stated, orbits 5-50, 10% 3D"
+                                if n == 2000 and scale == 1.0 else
+                                f"serving {n} requests (sample of the 2000-request stream), orbits "
+                                f"{5 * scale:g}-{50 * scale:g} (x{scale:g} of 5-50), 10% 3D"),
                    "arrivals": f"Poisson, {rate:.3f}/s = 1.5 x measured capacity {capacity:.3f}/s",
                    "hbm_budget_gb": 150, "max_slots": slots, "chunk": args.chunk},
         "latency": lat,

@@ -20,7 +20,11 @@
 //    the w slot of the radial sweep, the v slot of the azimuthal sweep) and
 //    umid *= pmid (evolve.cu:73, used by EOS 2 only) is dropped;
 //  * cs2(r) and nu(r) come from per-ring tables computed on the device with
-//    the same expressions.
+//    the same expressions;
+//  * the three parabolas of states and the three or four of remap run side
+//    by side, each with its own scratch arrays, where the reference runs
+//    them one after another through the same three (al/da/a6 over
+//    q/dx/tmp1); every value is the same, the barriers are shared.
 #pragma once
 
 #include <cuda_runtime.h>

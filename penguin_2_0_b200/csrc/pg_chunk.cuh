@@ -17,10 +17,17 @@ struct CellIn {
   double pol;    // polar angle (0 in 2D)
   double vrot;   // res_v / rad_cyl of the cell's ring
   double dvol0;  // Eulerian cell volume along the sweep
-  double sinpol; // sin(pol) of the cell (3D; the polar sweep's from a per-layer table)
-  double cospol; // cos(pol) of the cell (polar sweep)
-  double sinfz;  // sin, cos of the cell's left face angle (polar sweep, per-layer table)
-  double cosfz;
+  double sinpol; // sin(pol) of the cell (3D radial and azimuthal sweeps)
+  // polar sweep: the layer's sin/cos(centre), sin/cos(face) read where they
+  // are used, from lay[0], lay[nz], lay[2 nz], lay[3 nz] (the tables szc,
+  // czc, szf, czf at stride nz; plain loads, which a barrier keeps from
+  // being merged: nothing holds them in registers through the chain)
+  const double *lay;
+  int nz;
+  __device__ __forceinline__ double spol() const { return lay[0]; }
+  __device__ __forceinline__ double cpol() const { return lay[nz]; }
+  __device__ __forceinline__ double sfz() const { return lay[2 * nz]; }
+  __device__ __forceinline__ double cfz() const { return lay[3 * nz]; }
 };
 
 // x^2 where the reference writes pow(x, 2)
@@ -60,7 +67,7 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
     // whose sin and cos come from the per-layer table; the planet's angle
     // factor cos(azi + hdt v_rot - (p.y + hdt p.vy)) by angle addition from
     // the pencil's start-of-step cos and sin of azi - p.y
-    const double sp = c.sinfz, cp = c.cosfz;
+    const double sp = c.sfz(), cp = c.cfz();
     double grav = 0.0;
     if (ph.plnt) {
       double sd, cd;
@@ -119,6 +126,8 @@ __device__ __forceinline__ double centre_force(int n, double dt, double rad, dou
 // The ppmlr chain for one chunk.  All threads of the CTA call it (it has
 // barriers); cells n >= nmax take no part in any phase.  On return r, u, v
 // (and w when THREED) hold the Lagrange-remapped values for 6 <= n < nmax-6.
+// The polar sweep (AXIS 2) passes its layers' Eulerian paraset coefficients
+// in eul_par (5 per cell of the chunk) and c.lay for its layer tables.
 template <int AXIS, bool SPH, bool THREED, int EOS = 0, class SHM>
 __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, double FrRot,
                                           const CellIn &c, const Body &pl, const Phys &ph,
@@ -163,16 +172,11 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   // shared.
   const double hdt = 0.5 * dt;
   Par par;
-  if (AXIS == 2 && eul_par) {
-    // the polar sweep's Eulerian coefficients, one set per layer (k_tables;
-    // the polar sweep has no reference kernel whose bits it must follow)
-    if (n >= 1 && n < nmax - 1) {
-      const double *q = eul_par + 5 * n;
-      par.c0 = q[0]; par.c1 = q[1]; par.c2 = q[2]; par.c3 = q[3]; par.c4 = q[4];
-    }
-  } else {
-    paraset(n, 0, nmax, par, S.dx0, S.q, S.dx, S.tmp1);
-  }
+  // the polar sweep's Eulerian coefficients, one set per layer (k_tables;
+  // the polar sweep has no reference kernel whose bits it must follow), are
+  // read from the table where the parabolas use them
+  constexpr bool eul_tab = (AXIS == 2);
+  if (!eul_tab) paraset(n, 0, nmax, par, S.dx0, S.q, S.dx, S.tmp1);
   double ftot = 0.0;
   if (n >= 2 && n < nmax - 1) face_force<AXIS, SPH>(n, hdt, c, S, pl, ph, ftot);
   if (act) {
@@ -187,7 +191,8 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
     double *const al[3] = {S.q, S.s0, S.s3};
     double *const da[3] = {S.dx, S.s1, S.s4};
     double *const a6[3] = {S.tmp1, S.s2, S.s5};
-    parabola_n<3>(n, 0, nmax, flat, val, al, da, a6, par);
+    if (eul_tab) parabola_n<3>(n, 0, nmax, flat, val, al, da, a6, ParTab{eul_par + 5 * n});
+    else parabola_n<3>(n, 0, nmax, flat, val, al, da, a6, par);
     const double *cs = S.umid, *csfac = S.pmid;
     double sl[3] = {0.0, 0.0, 0.0}, sr[3] = {0.0, 0.0, 0.0};
     if (n >= 3 && n < nmax - 2) {
@@ -252,14 +257,15 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
       fto1 = centre_force<1, SPH>(n, 0.0, c.rad, c.azi, c.pol, c.sinpol, S, pl, ph);
       fto2 = centre_force<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, c.sinpol, S, pl, ph);
     } else {
-      fto1 = centre_force<2, SPH, true>(n, 0.0, c.rad, c.azi, c.pol, 0.0, S, pl, ph, S.cf0, c.sinpol, c.cospol);
+      const double spo = c.spol(), cpo = c.cpol();
+      fto1 = centre_force<2, SPH, true>(n, 0.0, c.rad, 0.0, 0.0, 0.0, S, pl, ph, S.cf0, spo, cpo);
       // sin, cos of the new centre angle from the layer's (xcl moved by a
       // fraction of a cell), and the planet's angle factor at t + dt from
       // the pencil's, by angle addition
       double se, ce, sd, cd;
       sincos_small(xcl - c.pol, se, ce);
-      sxcl = c.sinpol * ce + c.cospol * se;
-      const double cxcl = c.cospol * ce - c.sinpol * se;
+      sxcl = spo * ce + cpo * se;
+      const double cxcl = cpo * ce - spo * se;
       sincos_small(dt * (c.vrot - pl.vy), sd, cd);
       fto2 = centre_force<2, SPH, true>(n, dt, c.rad, 0.0, xcl, 0.0, S, pl, ph, S.cf0 * cd - S.sf0 * sd, sxcl, cxcl);
     }
@@ -288,13 +294,14 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
       double delx = xa - xa0n;
       double sw, cw;
       sincos_small(0.5 * dxn, sw, cw);
-      const double sc = (n < nmax - 3) ? sxcl : c.sinfz * cw + c.cosfz * sw;   // sin(xa0 + dxn / 2)
+      const double sfz = c.sfz(), cfz = c.cfz();
+      const double sc = (n < nmax - 3) ? sxcl : sfz * cw + cfz * sw;   // sin(xa0 + dxn / 2)
       dvol = 2.0 * sc * sw * c.rad;
-      if (delx == 0.0) vfac[n] = c.sinfz;                                     // sin(xa) = sin(xa0)
+      if (delx == 0.0) vfac[n] = sfz;                                 // sin(xa) = sin(xa0)
       else {
         double sh, ch;
         sincos_small(0.5 * delx, sh, ch);
-        sA = c.sinfz * ch + c.cosfz * sh;                                        // sin(xa0 + delx / 2)
+        sA = sfz * ch + cfz * sh;                                        // sin(xa0 + delx / 2)
         sB = sh;
         haveS = true;
         vfac[n] = 2.0 * sA * sB / delx;
@@ -333,7 +340,7 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
     else {
       double sh, ch;
       sincos_small(0.5 * d, sh, ch);
-      lvol = 2.0 * (c.sinfz * ch + c.cosfz * sh) * sh * c.rad;
+      lvol = 2.0 * (c.sfz() * ch + c.cfz() * sh) * sh * c.rad;
     }
   }
   double dxf = xa - xa0n;

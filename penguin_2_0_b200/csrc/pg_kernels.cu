@@ -103,7 +103,6 @@ __device__ __forceinline__ void sweep_x_body(ChunkShmData<NT> &S, int n, bool st
     c.azi = T.yc[j0];
     c.pol = THREED ? T.zc[k + NPAD] : 0.0;
     c.sinpol = THREED ? T.szc[k + NPAD] : 0.0;
-    c.cospol = 0.0;
     c.dvol0 = T.rxvol[row];
     // the pencil's planet angle factor at the start of the step, once
     if (n == 0) S.cf0 = ph.plnt ? planet_cosfac(c.azi, st.pl, 0.0) : 0.0;
@@ -119,7 +118,7 @@ __device__ __forceinline__ void sweep_x_body(ChunkShmData<NT> &S, int n, bool st
     bool ghost = (row < NPAD) || (row >= T.nr + NPAD);
     S.p[n] = ghost ? T.gp[rk] : (P.p0 ? P.p0[idx] : eos_p<EOS>(r, T.cs2[rk], ph));
   } else {
-    c.rad = 1.0; c.azi = 0.0; c.pol = 0.0; c.dvol0 = 1.0; c.vrot = 0.0; c.sinpol = 0.0; c.cospol = 0.0;
+    c.rad = 1.0; c.azi = 0.0; c.pol = 0.0; c.dvol0 = 1.0; c.vrot = 0.0; c.sinpol = 0.0;
   }
   __syncthreads();
   ppm_chunk<0, SPH, THREED, EOS>(S, n, lim, st.dt, st.frrot, c, st.pl, ph);
@@ -297,7 +296,6 @@ __device__ __forceinline__ void sweep_y_body(ChunkShmT<NT> &S, double *red, cons
     c.rad = rad_cyl;
     c.pol = THREED ? T.zc[k + NPAD] : 0.0;
     c.sinpol = THREED ? T.szc[k + NPAD] : 0.0;
-    c.cospol = 0.0;
     c.vrot = T.res_v[rk] / rad_cyl;
     c.azi = 0.0; c.dvol0 = 1.0;
     if (act) {
@@ -427,7 +425,8 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmData<NT> &S, int n, bool st
   CellIn c;
   c.rad = rad;
   c.azi = T.yc[j0];
-  c.pol = 0.0; c.vrot = 0.0; c.dvol0 = 1.0; c.sinpol = 0.0; c.cospol = 0.0; c.sinfz = 0.0; c.cosfz = 0.0;
+  c.pol = 0.0; c.vrot = 0.0; c.dvol0 = 1.0; c.sinpol = 0.0;
+  c.lay = T.szc; c.nz = nk + 2 * NPAD;
   // the pencil's planet angle factor at the start of the step, and its
   // sine (the polar chain's angle additions), once
   if (n == 0) {
@@ -472,10 +471,8 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmData<NT> &S, int n, bool st
       c.vrot = T.res_v[rkk] / rad_cyl;
     }
     c.pol = zc;
-    c.sinpol = T.szc[kr + NPAD];      // sin, cos of the layer's centre angle
-    c.cospol = T.czc[kr + NPAD];
-    c.sinfz = T.szf[kr + NPAD];       // and of its left face angle
-    c.cosfz = T.czf[kr + NPAD];
+    c.lay = T.szc + (kr + NPAD);      // sin, cos of the layer's centre angle
+    c.nz = nk + 2 * NPAD;             // and of its left face angle
     c.dvol0 = zvol * rad;
     S.xa0[n] = za;
     S.dx0[n] = dz;
@@ -519,7 +516,9 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmData<NT> &S, int n, bool st
     int inc = ctl.shift ? T.inc_j[rkk] : 0;
     const int jo = wrapm(j0 + inc, nphi);
     size_t o = (size_t)rkk * nphi + jo;
-    double r = S.r[n], vr = S.v[n], vp = S.w[n] / rad_cyl, vt = S.u[n];
+    // an interior cell's rad_cyl is radc (read again here rather than held
+    // through the chain)
+    double r = S.r[n], vr = S.v[n], vp = S.w[n] / T.radc[rkk], vt = S.u[n];
     if (ctl.fuse) {
       const double g = T.damp_g[rkk];
       if (g > 0.0) {
@@ -574,22 +573,28 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep_z(Tables T, Planes P, Phys p
 // at 3 CTAs/SM (56 registers, 33 resident warps against 30) take it to
 // 0.93 ms.  Pencils longer than 44 cells keep 4 per CTA.  An earlier 8-pencil
 // form at 2 CTAs/SM, before the bank padding, ran at 1.63 ms.
+// The 8-pencil kernel's shared blocks are sized for 44 cells (LIMZ; 52 KB
+// per CTA instead of 67), which leaves L1 room for the spill slots of its
+// 56-register threads; with the layer tables and paraset coefficients read
+// where they are used instead of held through the chain (4x fewer local
+// loads, 1.0 M per launch) that took the polar sweep from 0.781 to 0.707 ms.
 // Thread t works on cell t / PACK of pencil t % PACK,
 // and the PACK pencils of a CTA are consecutive azimuth columns of a ring,
 // so a warp's loads of one layer cover PACK adjacent doubles.  Pencils past
 // the last column repeat the last one without storing.
 constexpr int PZ_LIM = 56;
 constexpr int PZ8_THREADS = 352;   // 8 pencils of up to 44 cells, 3 CTAs per SM
-template <int PACK>
-using PzShm = ChunkShmT<PZ_LIM, 128 / PACK>;
-template <int PACK>
-constexpr int pz_shm_bytes() { return PACK * (int)sizeof(PzShm<PACK>); }
-template <int PACK, int MINB, int MAXT = PACK * PZ_LIM>
+constexpr int PZ8_LIM = PZ8_THREADS / 8;
+template <int PACK, int LIMZ = PZ_LIM>
+using PzShm = ChunkShmT<LIMZ, 128 / PACK>;
+template <int PACK, int LIMZ = PZ_LIM>
+constexpr int pz_shm_bytes() { return PACK * (int)sizeof(PzShm<PACK, LIMZ>); }
+template <int PACK, int MINB, int MAXT = PACK * PZ_LIM, int LIMZ = PZ_LIM>
 __global__ void __launch_bounds__(MAXT, MINB) k_sweep_z_packed(Tables T, Planes P, Phys ph, SweepCtl ctl, int ntop) {
-  // the PACK pencils' shared blocks, dynamic: 8 of them (67 KB) exceed the
+  // the PACK pencils' shared blocks, dynamic: 8 of them (52 KB) exceed the
   // 48 KiB a kernel may declare statically
   extern __shared__ __align__(16) unsigned char pz_shm[];
-  PzShm<PACK> *S = reinterpret_cast<PzShm<PACK> *>(pz_shm);
+  PzShm<PACK, LIMZ> *S = reinterpret_cast<PzShm<PACK, LIMZ> *>(pz_shm);
   StepIn st;
   if (!load_step(ctl, st)) return;
   const int p = threadIdx.x % PACK, n = threadIdx.x / PACK;
@@ -597,7 +602,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_z_packed(Tables T, Planes 
   int col = blockIdx.x * PACK + p;
   const bool store = col < npen;
   if (!store) col = npen - 1;
-  sweep_z_body<PZ_LIM>(S[p], n, store, T, P, ph, ctl, st, ntop, col / T.nphi, col % T.nphi, 0);
+  sweep_z_body<LIMZ>(S[p], n, store, T, P, ph, ctl, st, ntop, col / T.nphi, col % T.nphi, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -811,13 +816,14 @@ __device__ __forceinline__ double tree1024(double *list) {
   return list[0];
 }
 
-// Ring i of polar layer k; the last of the run's nblocks ring blocks to
-// finish adds up the run's partial sums.
+// Rings t0, t0 + tstep, ... (t = i + nr * k: ring i of polar layer k), each
+// summed on its own as one CTA of the reference sums it; the last of the
+// run's nblocks CTAs to finish adds up the run's partial sums.
 template <typename RT>
 __device__ __forceinline__ void reduce_body(const Tables &T, const RT *R, Body pl, const DevClock *clk,
                                             double exclude, int mode, int plnt, double p_alpha, int ndim,
                                             double *ring_part, unsigned int *counter, double *out,
-                                            double *hist_row, int i, int k, unsigned nblocks,
+                                            double *hist_row, int t0, int tstep, unsigned nblocks,
                                             bool every_step = false) {
   __shared__ double list[1024];
   __shared__ bool is_last;
@@ -826,51 +832,54 @@ __device__ __forceinline__ void reduce_body(const Tables &T, const RT *R, Body p
     if (every_step && clk->halted) return;
     pl = clk->planet;
   }
-  const int row = i + NPAD, rk = k * T.nrg + row;
-  const int nphi = T.nphi;
-  const size_t base = (size_t)rk * nphi;
   const int tt = threadIdx.x;
-  const int rot = T.rot_j[rk];
-  const double rad = T.rxc[row], xvol = T.rxvol[row];
-  const double zvol = (ndim == 3) ? T.zvol[k + NPAD] : 1.0;
-  // FP32 planes hold Sigma - S_bg(ring)
-  const double r_off = (sizeof(RT) == 4) ? T.sbg[rk] : 0.0;
-  const int loop = nphi / 1024 + (nphi % 1024 != 0);
-  double val = 0.0;
-  for (int l = 0; l < loop; l++) {
-    int j = tt + 1024 * l;   // storage index
-    double v = 0.0;
-    if (j < nphi) {
-      int j0 = wrap1(j + rot, nphi);
-      double phi = T.yc[j0];
-      double r = r_off + (double)R[base + j0];
-      if (plnt) {
-        if (mode == 0) v = r * xvol * T.yvol[j0] * zvol;
-        else if (ndim == 2 && (mode == 8 || mode == 9)) {
-          if ((rad - pl.x) * (rad - pl.x) + rad * rad * (phi - pl.y) * (phi - pl.y) > exclude * exclude) {
-            if (mode == 8) {
-              double t = -grav_rad_cyl(rad, phi, 0.0, pl, 0.0);
-              t *= (r - pow(rad, -p_alpha)) * xvol * T.yvol[j0];
-              v = t;
-            } else {
-              double t = -grav_azi_cyl(rad, phi, 0.0, pl, 0.0);
-              t *= rad * (r - pow(rad, -p_alpha)) * xvol * T.yvol[j0];
-              v = t;
+  for (int rt = t0; rt < T.nr * T.nk; rt += tstep) {
+    const int i = rt % T.nr, k = rt / T.nr;
+    const int row = i + NPAD, rk = k * T.nrg + row;
+    const int nphi = T.nphi;
+    const size_t base = (size_t)rk * nphi;
+    const int rot = T.rot_j[rk];
+    const double rad = T.rxc[row], xvol = T.rxvol[row];
+    const double zvol = (ndim == 3) ? T.zvol[k + NPAD] : 1.0;
+    // FP32 planes hold Sigma - S_bg(ring)
+    const double r_off = (sizeof(RT) == 4) ? T.sbg[rk] : 0.0;
+    const int loop = nphi / 1024 + (nphi % 1024 != 0);
+    double val = 0.0;
+    for (int l = 0; l < loop; l++) {
+      int j = tt + 1024 * l;   // storage index
+      double v = 0.0;
+      if (j < nphi) {
+        int j0 = wrap1(j + rot, nphi);
+        double phi = T.yc[j0];
+        double r = r_off + (double)R[base + j0];
+        if (plnt) {
+          if (mode == 0) v = r * xvol * T.yvol[j0] * zvol;
+          else if (ndim == 2 && (mode == 8 || mode == 9)) {
+            if ((rad - pl.x) * (rad - pl.x) + rad * rad * (phi - pl.y) * (phi - pl.y) > exclude * exclude) {
+              if (mode == 8) {
+                double t = -grav_rad_cyl(rad, phi, 0.0, pl, 0.0);
+                t *= (r - pow(rad, -p_alpha)) * xvol * T.yvol[j0];
+                v = t;
+              } else {
+                double t = -grav_azi_cyl(rad, phi, 0.0, pl, 0.0);
+                t *= rad * (r - pow(rad, -p_alpha)) * xvol * T.yvol[j0];
+                v = t;
+              }
             }
           }
+        } else {
+          v = r * xvol * T.yvol[j0] * zvol;
         }
-      } else {
-        v = r * xvol * T.yvol[j0] * zvol;
       }
+      list[tt] = v;
+      __syncthreads();
+      double s = tree1024(list);
+      if (tt == 0) val += s;
+      __syncthreads();
     }
-    list[tt] = v;
-    __syncthreads();
-    double s = tree1024(list);
-    if (tt == 0) val += s;
-    __syncthreads();
+    if (tt == 0) ring_part[i + T.nr * k] = val;
   }
   if (tt == 0) {
-    ring_part[i + T.nr * k] = val;
     __threadfence();
     unsigned int prev = atomicAdd(counter, 1u);
     is_last = (prev == nblocks - 1);
@@ -924,7 +933,7 @@ __global__ void __launch_bounds__(1024) k_reduce(Tables T, const RT *R, Body pl,
                                                  int ndim, double *ring_part, unsigned int *counter,
                                                  double *out, double *hist_row) {
   reduce_body<RT>(T, R, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter, out, hist_row,
-                  blockIdx.x, blockIdx.y, gridDim.x * gridDim.y);
+                  blockIdx.x, gridDim.x, gridDim.x);
 }
 
 // moving planet: the disk's radial (mode 8) and azimuthal (mode 9) force
@@ -934,7 +943,7 @@ __global__ void __launch_bounds__(1024) k_reduce_forces(Tables T, const RT *R, D
                                                         double p_alpha, int ndim, double *ring_part,
                                                         unsigned int *counter) {
   reduce_body<RT>(T, R, Body{}, clk, 0.0, mode, 1, p_alpha, ndim, ring_part, counter,
-                  mode == 8 ? &clk->f8 : &clk->f9, nullptr, blockIdx.x, blockIdx.y, gridDim.x * gridDim.y, true);
+                  mode == 8 ? &clk->f8 : &clk->f9, nullptr, blockIdx.x, gridDim.x, gridDim.x, true);
 }
 
 // append a diagnostics row when this step prints (main.cu:414-428)
@@ -1298,7 +1307,7 @@ __global__ void __launch_bounds__(1024) kb_reduce(BatchQueue q, int mode) {
   else R = (const RT *)b.PX.r;
   double *out = (mode == 0) ? &b.clk->mass : &b.clk->torque;
   reduce_body<RT>(b.T, R, Body{}, b.clk, 0.0, mode, mode == 9 ? 1 : b.plnt, b.p_alpha, 2, b.ring_part, b.counter,
-                  out, nullptr, blockIdx.x - q.start[r], 0, (unsigned)b.T.nr);
+                  out, nullptr, blockIdx.x - q.start[r], b.T.nr, (unsigned)b.T.nr);
 }
 
 template <int MINB>
@@ -1495,8 +1504,8 @@ static void sweep_z_t(const Tables &T, const Planes &P, const Phys &ph, const Sw
     if (T.zpack && ch.loop == 1 && !ch.stuck && ch.lim_last <= PZ_LIM) {
       int npen = T.nr * T.nphi;
       if (8 * ch.lim_last <= PZ8_THREADS)    // whole warps: 8 pencils of 44 cells (kmax 32) are 11
-        k_sweep_z_packed<8, 3, PZ8_THREADS><<<(npen + 7) / 8, 8 * ch.lim_last, pz_shm_bytes<8>(), s>>>(T, P, ph, c,
-                                                                                                        ntop);
+        k_sweep_z_packed<8, 3, PZ8_THREADS, PZ8_LIM>
+            <<<(npen + 7) / 8, 8 * ch.lim_last, pz_shm_bytes<8, PZ8_LIM>(), s>>>(T, P, ph, c, ntop);
       else
         k_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, pz_shm_bytes<4>(), s>>>(T, P, ph, c, ntop);
       return;
@@ -1526,11 +1535,12 @@ int sweep_launches(const Chunking &ch) { return (ch.stuck || ch.loop == 1) ? 1 :
 // form, and prefer the largest shared-memory carveout so that 3 CTAs of it
 // (201 KB) fit on an SM.
 int setup_device() {
-  cudaError_t e = cudaFuncSetAttribute(k_sweep_z_packed<8, 3, PZ8_THREADS>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, pz_shm_bytes<8>());
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_sweep_z_packed<8, 3, PZ8_THREADS>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             100);
+  // 8 polar pencils of up to 44 cells: 52 KB of shared blocks per CTA.  No
+  // carveout preference: the driver's choice leaves L1 room for the spill
+  // slots of 3 CTAs (polar sweep 0.707 ms on the 128x1024x32 disk, against
+  // 0.715 at a 72 % carveout and 0.728 at 100 %)
+  cudaError_t e = cudaFuncSetAttribute(k_sweep_z_packed<8, 3, PZ8_THREADS, PZ8_LIM>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, pz_shm_bytes<8, PZ8_LIM>());
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_sweep_z_packed<4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              pz_shm_bytes<4>());
@@ -1581,19 +1591,32 @@ void cfl_clk(const Tables &T, const double *r, const double *u, const double *v,
   k_cfl_clk<<<grid, 256, 0, s>>>(T, r, u, v, w, ph, clk, 3, 1);
 }
 
+// The ring sums run on two 1024-thread CTAs per SM, each taking every
+// grid-th ring: most steps print nothing and every CTA returns at once, so
+// a grid of one CTA per ring would only pay for starting them.
+static int reduce_grid(const Tables &T) {
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm <= 0) nsm = 148;
+  }
+  const int rings = T.nr * T.nk;
+  return rings < 2 * nsm ? rings : 2 * nsm;
+}
+
 void reduce(const Tables &T, const double *r, const Body &pl, const DevClock *clk, double exclude,
             int mode, int plnt, double p_alpha, int ndim, double *ring_part, unsigned int *counter,
             double *out, double *hist_row, cudaStream_t s) {
-  dim3 grid(T.nr, T.nk);
-  k_reduce<double><<<grid, 1024, 0, s>>>(T, r, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter,
+  k_reduce<double><<<reduce_grid(T), 1024, 0, s>>>(T, r, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter,
                                          out, hist_row);
 }
 
 void reduce32(const Tables &T, const float *r, const Body &pl, const DevClock *clk, double exclude, int mode,
               int plnt, double p_alpha, int ndim, double *ring_part, unsigned int *counter, double *out,
               cudaStream_t s) {
-  dim3 grid(T.nr, T.nk);
-  k_reduce<float><<<grid, 1024, 0, s>>>(T, r, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter,
+  k_reduce<float><<<reduce_grid(T), 1024, 0, s>>>(T, r, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter,
                                         out, nullptr);
 }
 
@@ -1610,7 +1633,7 @@ void poststep_kick(DevClock *clk, cudaStream_t s) {
 }
 void reduce_forces(const Tables &T, const void *r, int fp32, DevClock *clk, double p_alpha, int ndim,
                    double *ring_part, unsigned int *counter, cudaStream_t s) {
-  dim3 grid(T.nr, T.nk);
+  const int grid = reduce_grid(T);
   for (int mode : {8, 9}) {
     if (fp32)
       k_reduce_forces<float><<<grid, 1024, 0, s>>>(T, (const float *)r, clk, mode, p_alpha, ndim, ring_part, counter);

@@ -98,6 +98,15 @@ __device__ __forceinline__ void riemann_isentropic(double pl, double rl, double 
 }
 
 struct Par { double c0, c1, c2, c3, c4; };
+// paraset coefficients read where they are used from a table (q[0..4]),
+// with plain loads that a barrier keeps apart, instead of held in registers
+struct ParTab { const double *q; };
+template <int I>
+__device__ __forceinline__ double par_c(const Par &p) {
+  return I == 0 ? p.c0 : I == 1 ? p.c1 : I == 2 ? p.c2 : I == 3 ? p.c3 : p.c4;
+}
+template <int I>
+__device__ __forceinline__ double par_c(const ParTab &p) { return p.q[I]; }
 
 // Shared arrays of one chunk: the sweep kernel's (ppm.cu:38-39) and
 // ppmlr's (ppmlr.cu:7-10).  q only serves as parabola storage (al) because
@@ -354,17 +363,18 @@ __device__ __forceinline__ void parabola(int n, int nmin, int nmax, double flat,
 // instead of one per phase and field.  A field's values and its own a6 are
 // reloaded from shared memory after a barrier (same bits) so that only ar
 // stays in a register across one.
-template <int NF>
+template <int NF, class PS>
 __device__ __forceinline__ void parabola_n(int n, int nmin, int nmax, double flat, const double *const *val,
                                            double *const *al, double *const *da, double *const *a6,
-                                           const Par &par) {
+                                           const PS &par) {
   if (n >= nmin + 1 && n < nmax - 1) {
+    const double c3 = par_c<3>(par), c4 = par_c<4>(par);
 #pragma unroll
     for (int f = 0; f < NF; f++) {
       const double a = val[f][n];
       const double da_r = val[f][n + 1] - a;
       const double da_l = a - val[f][n - 1];
-      double t1 = par.c3 * da_r + par.c4 * da_l;
+      double t1 = c3 * da_r + c4 * da_l;
       if (t1 < 0.0) t1 = -min3(-t1, 2.0 * fabs(da_l), 2.0 * fabs(da_r));
       else          t1 = min3(t1, 2.0 * fabs(da_l), 2.0 * fabs(da_r));
       if (da_l * da_r < 0.0) t1 = 0.0;
@@ -374,12 +384,13 @@ __device__ __forceinline__ void parabola_n(int n, int nmin, int nmax, double fla
   __syncthreads();
   double ar[NF];
   if (n >= nmin + 1 && n < nmax - 2) {
+    const double c0 = par_c<0>(par), c1 = par_c<1>(par), c2 = par_c<2>(par);
 #pragma unroll
     for (int f = 0; f < NF; f++) {
       const double a = val[f][n];
       const double da_r = val[f][n + 1] - a;
       const double t1 = a6[f][n];
-      ar[f] = a + par.c0 * da_r + par.c1 * a6[f][n + 1] + par.c2 * t1;
+      ar[f] = a + c0 * da_r + c1 * a6[f][n + 1] + c2 * t1;
       al[f][n + 1] = ar[f];
     }
   }

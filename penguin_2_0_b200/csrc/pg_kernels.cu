@@ -1478,6 +1478,15 @@ template <int EOS>
 static void sweep_y_t(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
   const Chunking &ch = T.cy;
   const int occ8 = T.occ8;
+  if (!ch.stuck && cta_for(ch.lim_last) == 128) {
+    // a last chunk of more than 64 cells takes the full chunks' 128-thread
+    // CTAs: one launch for all of them (the body gives chunk loop-1 its
+    // lim_last), whose CTAs fill the tail of the full chunks' last wave
+    dim3 grid(ch.loop, T.nr, T.nk);
+    if (ndim == 3) launch_y<true, true, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
+    else launch_y<false, false, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
+    return;
+  }
   int full = ch.stuck ? ch.loop : ch.loop - 1;
   if (full > 0) {
     dim3 grid(full, T.nr, T.nk);
@@ -1528,6 +1537,11 @@ void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c
 
 // kernels launched by one sweep_* call
 int sweep_launches(const Chunking &ch) { return (ch.stuck || ch.loop == 1) ? 1 : 2; }
+// the FP64 azimuthal sweep runs its last chunk in the same launch when it
+// takes 128-thread CTAs too (sweep_y_t)
+int sweep_y_launches(const Chunking &ch) {
+  return (ch.stuck || ch.loop == 1 || cta_for(ch.lim_last) == 128) ? 1 : 2;
+}
 
 // Per-device kernel attributes, set with the device current before the first
 // launch (pg_create): the packed polar kernels take their shared blocks as

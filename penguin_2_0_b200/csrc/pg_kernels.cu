@@ -195,7 +195,8 @@ __global__ void __launch_bounds__(4 * LIM, MINB) k_sweep_x_packed(Tables T, Plan
   sweep_x_body<SPH, THREED, LIM>(S[p], n, store, T, P, ph, ctl, st, col % T.nphi, T.cx.loop - 1, col / T.nphi);
 }
 
-// Full radial chunks of PACK adjacent columns per CTA (128 * PACK threads,
+// Full radial chunks (and a last chunk of more than 64 cells, in the same
+// launch) of PACK adjacent columns per CTA (128 * PACK threads,
 // thread t on cell t / PACK of column t % PACK): a warp's loads and stores of
 // one ring cover PACK adjacent doubles, where one column per CTA touches a
 // separate 32-byte sector per cell.  Columns past the last one repeat it
@@ -1425,13 +1426,17 @@ static void sweep_x_t(const Tables &T, const Planes &P, const Phys &ph, const Sw
   const Chunking &ch = T.cx;
   const int occ8 = T.occ8;
   int full = ch.stuck ? ch.loop : ch.loop - 1;
+  // a last chunk of more than 64 cells runs in the full chunks' launch (the
+  // body gives chunk loop-1 its lim_last), whose tail it fills
+  const bool merge = !ch.stuck && full > 0 && ch.lim_last > 64;
+  if (merge) full = ch.loop;
   if (full > 0) {
     bool done = false;
     if constexpr (EOS == 0) {
       // a stuck last chunk (imax % 116 == 0) keeps the one-column kernel
       const int xp = (ch.stuck || !occ8) ? 1 : T.xpack;
       if (xp == 2 || xp == 4) {
-        dim3 grid((T.nphi + xp - 1) / xp, ch.loop - 1, T.nk);
+        dim3 grid((T.nphi + xp - 1) / xp, full, T.nk);
         if (xp == 2) {
           if (ndim == 3) k_sweep_x_cols<true, true, 2, 4><<<grid, 2 * ARR, px_shm_bytes<2>(), s>>>(T, P, ph, c);
           else k_sweep_x_cols<false, false, 2, 4><<<grid, 2 * ARR, px_shm_bytes<2>(), s>>>(T, P, ph, c);
@@ -1448,7 +1453,7 @@ static void sweep_x_t(const Tables &T, const Planes &P, const Phys &ph, const Sw
       else launch_x<false, false, EOS>(128, occ8, grid, 0, T, P, ph, c, s);
     }
   }
-  if (!ch.stuck) {
+  if (!ch.stuck && !merge) {
     if constexpr (EOS == 0) {
       if (T.zpack && ch.lim_last <= PX_LIM) {
         int npen = T.nphi * T.nk, blocks = (npen + 3) / 4, nt = 4 * ch.lim_last;
@@ -1537,6 +1542,9 @@ void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c
 
 // kernels launched by one sweep_* call
 int sweep_launches(const Chunking &ch) { return (ch.stuck || ch.loop == 1) ? 1 : 2; }
+// the FP64 radial sweep runs a last chunk of more than 64 cells in the full
+// chunks' launch (sweep_x_t)
+int sweep_x_launches(const Chunking &ch) { return (ch.stuck || ch.loop == 1 || ch.lim_last > 64) ? 1 : 2; }
 // the FP64 azimuthal sweep runs its last chunk in the same launch when it
 // takes 128-thread CTAs too (sweep_y_t)
 int sweep_y_launches(const Chunking &ch) {

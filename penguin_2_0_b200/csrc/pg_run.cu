@@ -571,7 +571,9 @@ static pgd::SweepCtl host_ctl(double dt, const pg_body *pl, double frrot) {
   return c;
 }
 
-static int nx(pg_run *run) { return pgk::sweep_launches(run->T.cx); }
+static int nx(pg_run *run) {
+  return run->fp32 ? pgk::sweep_launches(run->T.cx) : pgk::sweep_x_launches(run->T.cx);
+}
 static int ny(pg_run *run) {
   return run->fp32 ? pgk::sweep_launches(run->T.cy) : pgk::sweep_y_launches(run->T.cy);
 }

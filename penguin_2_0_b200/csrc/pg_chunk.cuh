@@ -18,9 +18,10 @@ struct CellIn {
   double vrot;   // res_v / rad_cyl of the cell's ring
   double dvol0;  // Eulerian cell volume along the sweep
   double sinpol; // sin(pol) of the cell (3D radial and azimuthal sweeps)
-  // polar sweep: the layer's sin/cos(centre), sin/cos(face) read where they
-  // are used, from lay[0], lay[nz], lay[2 nz], lay[3 nz] (the tables szc,
-  // czc, szf, czf at stride nz; plain loads, which a barrier keeps from
+  // polar sweep: the layer's sin/cos(centre), sin/cos(face) and the
+  // reciprocals 1/sin(centre), 1/sin(face), 1/dz read where they are used,
+  // from lay[0], lay[nz], ..., lay[6 nz] (the tables szc, czc, szf, czf,
+  // iszc, iszf, idz at stride nz; plain loads, which a barrier keeps from
   // being merged: nothing holds them in registers through the chain)
   const double *lay;
   int nz;
@@ -28,6 +29,9 @@ struct CellIn {
   __device__ __forceinline__ double cpol() const { return lay[nz]; }
   __device__ __forceinline__ double sfz() const { return lay[2 * nz]; }
   __device__ __forceinline__ double cfz() const { return lay[3 * nz]; }
+  __device__ __forceinline__ double iszc() const { return lay[4 * nz]; }   // 1 / sin(centre)
+  __device__ __forceinline__ double iszf() const { return lay[5 * nz]; }   // 1 / sin(face)
+  __device__ __forceinline__ double idz() const { return lay[6 * nz]; }    // 1 / dz
 };
 
 // x^2 where the reference writes pow(x, 2)
@@ -72,9 +76,9 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
     if (ph.plnt) {
       double sd, cd;
       sincos_small(hdt * (c.vrot - pl.vy), sd, cd);
-      grav = grav_pol_sph_cf(c.rad, S.cf0 * cd - S.sf0 * sd, sp, cp, pl);
+      grav = grav_pol_sph_plm(c.rad, S.cf0 * cd - S.sf0 * sd, sp, cp, S.plm, pl);
     }
-    double irc = 1.0 / (c.rad * sp);
+    const double irc = c.iszf() * S.irad;   // 1 / (r sin(face)) from the pencil's and layer's reciprocals
     double f = grav;
     f += __dmul_rn(sq(0.5 * (S.w[n] + S.w[n - 1])) * cp, __dmul_rn(__dmul_rn(irc, irc), irc));
     ftot = f;
@@ -88,7 +92,8 @@ __device__ __forceinline__ void face_force(int n, double hdt, const CellIn &c, c
 template <int AXIS, bool SPH, bool CF0 = false, class SHM>
 __device__ __forceinline__ double centre_force(int n, double dt, double rad, double azi, double pol,
                                                double sinpol, const SHM &S, const Body &pl, const Phys &ph,
-                                               double cf0 = 0.0, double sp = 0.0, double cp = 0.0) {
+                                               double cf0 = 0.0, double sp = 0.0, double cp = 0.0,
+                                               double irc_in = 0.0) {
   if (AXIS == 0) {
     double grav;
     const double ir = 1.0 / rad, ir2 = __dmul_rn(ir, ir), ir3 = __dmul_rn(ir2, ir);
@@ -113,10 +118,12 @@ __device__ __forceinline__ double centre_force(int n, double dt, double rad, dou
     if (!SPH) return ph.plnt ? grav_azi_cyl(rad, azi, pol, pl, dt) : 0.0;
     return ph.plnt ? grav_azi_sph_s(rad, azi, sinpol, pl, dt) : 0.0;
   } else {
+    // the polar sweep's form (CF0): the planet's reduced mass and
+    // 1 / (r sin) from the caller (irc_in)
     (void)pol;
     double grav = 0.0;
-    if (ph.plnt) grav = CF0 ? grav_pol_sph_cf(rad, cf0, sp, cp, pl) : grav_pol_sph_s(rad, azi, sp, cp, pl, dt);
-    double irc = 1.0 / (rad * sp);
+    if (ph.plnt) grav = CF0 ? grav_pol_sph_plm(rad, cf0, sp, cp, S.plm, pl) : grav_pol_sph_s(rad, azi, sp, cp, pl, dt);
+    const double irc = CF0 ? irc_in : 1.0 / (rad * sp);
     double f = grav;
     f += __dmul_rn(S.w[n] * S.w[n] * cp, __dmul_rn(__dmul_rn(irc, irc), irc));
     return f;
@@ -180,9 +187,14 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
   double ftot = 0.0;
   if (n >= 2 && n < nmax - 1) face_force<AXIS, SPH>(n, hdt, c, S, pl, ph, ftot);
   if (act) {
-    double cs = hdt * sqrt(ph.gam * S.p[n] / S.r[n]) / S.dx0[n];
-    if (AXIS == 1) cs /= c.rad;
-    if (AXIS == 2) cs /= c.rad;
+    double cs;
+    if (AXIS == 2) {
+      // the polar sweep's dx0 is its layer's dz: 1 / (dz r) from reciprocals
+      cs = hdt * sqrt(ph.gam * S.p[n] / S.r[n]) * (c.idz() * S.irad);
+    } else {
+      cs = hdt * sqrt(ph.gam * S.p[n] / S.r[n]) / S.dx0[n];
+      if (AXIS == 1) cs /= c.rad;
+    }
     S.umid[n] = cs;
     S.pmid[n] = 1.0 - kFourthd * cs;
   }
@@ -258,7 +270,8 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
       fto2 = centre_force<1, SPH>(n, dt, c.rad, xcl + dt * c.vrot, c.pol, c.sinpol, S, pl, ph);
     } else {
       const double spo = c.spol(), cpo = c.cpol();
-      fto1 = centre_force<2, SPH, true>(n, 0.0, c.rad, 0.0, 0.0, 0.0, S, pl, ph, S.cf0, spo, cpo);
+      fto1 = centre_force<2, SPH, true>(n, 0.0, c.rad, 0.0, 0.0, 0.0, S, pl, ph, S.cf0, spo, cpo,
+                                        c.iszc() * S.irad);
       // sin, cos of the new centre angle from the layer's (xcl moved by a
       // fraction of a cell), and the planet's angle factor at t + dt from
       // the pencil's, by angle addition
@@ -267,7 +280,8 @@ __device__ __forceinline__ void ppm_chunk(SHM &S, int n, int nmax, double dt, do
       sxcl = spo * ce + cpo * se;
       const double cxcl = cpo * ce - spo * se;
       sincos_small(dt * (c.vrot - pl.vy), sd, cd);
-      fto2 = centre_force<2, SPH, true>(n, dt, c.rad, 0.0, xcl, 0.0, S, pl, ph, S.cf0 * cd - S.sf0 * sd, sxcl, cxcl);
+      fto2 = centre_force<2, SPH, true>(n, dt, c.rad, 0.0, xcl, 0.0, S, pl, ph, S.cf0 * cd - S.sf0 * sd, sxcl, cxcl,
+                                        1.0 / (c.rad * sxcl));
     }
   }
   __syncthreads();

@@ -433,6 +433,9 @@ __device__ __forceinline__ void sweep_z_body(ChunkShmData<NT> &S, int n, bool st
   if (n == 0) {
     S.cf0 = ph.plnt ? planet_cosfac(c.azi, st.pl, 0.0) : 0.0;
     S.sf0 = ph.plnt ? sin(c.azi - (st.pl.y + 0.0 * st.pl.vy)) : 0.0;
+    S.irad = 1.0 / rad;
+    const double stm = 1.0 / (1.0 + st.pl.m);
+    S.plm = st.pl.m * stm;
   }
   double rad_cyl = 1.0;
   size_t idx = 0;
@@ -615,11 +618,16 @@ __global__ void k_tables(Tables T, Phys ph, int ndim, double kill_rin, double ki
   int n = T.nk * T.nrg;
   const int nz = T.nk + 2 * NPAD;
   if (t < nz) {
-    // sin, cos of every polar layer's centre angle (ghost layers included)
+    // sin, cos of every polar layer's centre and face angles (ghost layers
+    // included), and the reciprocals the polar sweep multiplies by where its
+    // divisions by r sin(theta) and r dz would otherwise repeat per cell
     const_cast<double *>(T.szc)[t] = sin(T.zc[t]);
     const_cast<double *>(T.czc)[t] = cos(T.zc[t]);
     const_cast<double *>(T.szf)[t] = sin(T.z[t]);
     const_cast<double *>(T.czf)[t] = cos(T.z[t]);
+    const_cast<double *>(T.iszc)[t] = 1.0 / sin(T.zc[t]);
+    const_cast<double *>(T.iszf)[t] = 1.0 / sin(T.z[t]);
+    const_cast<double *>(T.idz)[t] = 1.0 / T.dz[t];
     // the polar sweep's Eulerian paraset coefficients: every polar pencil
     // has the layers' widths dz, so they are one set per layer (c0..c2 where
     // dz[t + 2] exists, c3 and c4 where dz[t + 1] does)

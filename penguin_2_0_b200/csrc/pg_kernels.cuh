@@ -38,6 +38,7 @@ struct Tables {
   const double *z, *dz, *zvol, *zc;             // [nk + 12]: 6 ghost layers each side
   const double *szc, *czc;                      // [nk + 12]: sin(zc), cos(zc) (k_tables)
   const double *szf, *czf;                      // [nk + 12]: sin(z), cos(z) of the layer faces
+  const double *iszc, *iszf, *idz;              // [nk + 12]: 1/sin(zc), 1/sin(z), 1/dz (polar sweep)
   const double *zpar;                           // [5 (nk + 12)]: Eulerian paraset c0..c4 per layer (k_tables)
   const double *nug;                            // [12 nr]: nu of the polar ghost layers (6 below, 6 above) per ring
   const double *val_r, *val_u, *val_v;          // [nk*nrg] damping / FARGO targets

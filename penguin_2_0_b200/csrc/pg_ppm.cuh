@@ -124,6 +124,9 @@ struct ChunkShmData {
   double cf0;
   // sin(phi - phi_planet) at the start of the step (polar pencils, cell 0)
   double sf0;
+  // polar pencils (cell 0): 1 / r of the ring, and the planet's reduced
+  // mass p.m / (1 + p.m) of its forces
+  double irad, plm;
 };
 
 // Bytes that bring a per-pencil shared block to TO mod 128.  Kernels that
@@ -242,6 +245,15 @@ __device__ __forceinline__ double grav_pol_sph_cf(double rad, double cosfac, dou
   double plm = p.m * stm;
   double plx = p.x;
   (void)stm;
+  double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac * sinpol;
+  Rp = sqrt(Rp + p.rs * p.rs);
+  return plm * plx * cosfac * cospol / (Rp * Rp * Rp) - plm * cosfac * cospol / (sinpol * plx * plx);
+}
+// grav_pol_sph_cf with the reduced mass p.m / (1 + p.m) formed once by the
+// caller (the polar sweep, once per pencil)
+__device__ __forceinline__ double grav_pol_sph_plm(double rad, double cosfac, double sinpol, double cospol,
+                                                   double plm, const Body &p) {
+  double plx = p.x;
   double Rp = rad * rad + plx * plx - 2.0 * plx * rad * cosfac * sinpol;
   Rp = sqrt(Rp + p.rs * p.rs);
   return plm * plx * cosfac * cospol / (Rp * Rp * Rp) - plm * cosfac * cospol / (sinpol * plx * plx);

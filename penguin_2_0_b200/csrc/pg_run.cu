@@ -190,7 +190,7 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
   int nrg = run->nrg, nphi = run->nphi, nk = run->nk, nr = run->nr;
   size_t nring = (size_t)nk * nrg;
   size_t nz = (size_t)nk + 2 * NPAD;
-  run->tab_elems = 4 * (size_t)nrg + 10 * nring + 4 * (size_t)nphi + 13 * nz + (size_t)2 * NPAD * nr * 4 +
+  run->tab_elems = 4 * (size_t)nrg + 10 * nring + 4 * (size_t)nphi + 16 * nz + (size_t)2 * NPAD * nr * 4 +
                    (size_t)2 * NPAD * nr;
   if (cudaMalloc(&run->tab, run->tab_elems * sizeof(double)) != cudaSuccess) return bail(PG_ERR_NOMEM);
   if (cudaMalloc(&run->itab, 2 * nring * sizeof(int)) != cudaSuccess) return bail(PG_ERR_NOMEM);
@@ -227,7 +227,10 @@ int pg_create(const pg_params *p, int device, pg_run **out) {
   // rot_v shares the block below (10th ring table)
   T.y = t; t += nphi; T.dy = t; t += nphi; T.yvol = t; t += nphi; T.yc = t; t += nphi;
   T.z = t; t += nz; T.dz = t; t += nz; T.zvol = t; t += nz; T.zc = t; t += nz;
+  // szc, czc, szf, czf, iszc, iszf, idz consecutive at stride nz: the polar
+  // sweep reads them as lay[0], lay[nz], ... from one pointer per layer
   T.szc = t; t += nz; T.czc = t; t += nz; T.szf = t; t += nz; T.czf = t; t += nz;
+  T.iszc = t; t += nz; T.iszf = t; t += nz; T.idz = t; t += nz;
   T.zpar = t; t += 5 * nz;
   T.nug = t; t += (size_t)2 * NPAD * nr;
   T.tg = t; t += (size_t)2 * NPAD * nr * 4;
@@ -1186,7 +1189,7 @@ extern "C" size_t pg_run_device_bytes(const pg_params *p) {
   size_t es = (p->precision == 1) ? sizeof(float) : sizeof(double);
   size_t b = 2 * (size_t)nf * up(pe * es);
   if (p->precision != 1) b += up(pe * sizeof(double));                         // p0
-  b += up((4 * nrg + 10 * nring + 4 * nphi + 13 * nz + 2 * NPAD * nr * 4 + 2 * NPAD * nr) * sizeof(double));
+  b += up((4 * nrg + 10 * nring + 4 * nphi + 16 * nz + 2 * NPAD * nr * 4 + 2 * NPAD * nr) * sizeof(double));
   b += up(2 * nring * sizeof(int)) + 3 * up(nring * sizeof(double));           // itab, rot_v, vbg, sbg
   b += up(nr * nk * sizeof(double)) + up(4) + up(32) + up(8) + up(sizeof(pgd::DevClock));
   b += up((size_t)4096 * pgd::HIST_COLS * sizeof(double));

@@ -1534,11 +1534,13 @@ static void sweep_z_t(const Tables &T, const Planes &P, const Phys &ph, const Sw
     }
   }
   int full = ch.stuck ? ch.loop : ch.loop - 1;
+  const bool merge = !ch.stuck && full > 0 && ch.lim_last > 64;   // as in sweep_x_t
+  if (merge) full = ch.loop;
   if (full > 0) {
     dim3 grid(T.nr, T.nphi, full);
     launch_z<EOS>(128, T.occ8, grid, 0, ntop, T, P, ph, c, s);
   }
-  if (!ch.stuck) {
+  if (!ch.stuck && !merge) {
     dim3 grid(T.nr, T.nphi, 1);
     launch_z<EOS>(cta_for(ch.lim_last), T.occ8, grid, ch.loop - 1, ntop, T, P, ph, c, s);
   }
@@ -1548,22 +1550,15 @@ void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c
   else sweep_z_t<0>(T, P, ph, c, ntop, s);
 }
 
-// kernels launched by one sweep_* call
-int sweep_launches(const Chunking &ch) { return (ch.stuck || ch.loop == 1) ? 1 : 2; }
-// the FP64 radial sweep runs a last chunk of more than 64 cells in the full
-// chunks' launch (sweep_x_t)
-int sweep_x_launches(const Chunking &ch) { return (ch.stuck || ch.loop == 1 || ch.lim_last > 64) ? 1 : 2; }
-// the FP64 azimuthal sweep runs its last chunk in the same launch when it
-// takes 128-thread CTAs too (sweep_y_t)
-int sweep_y_launches(const Chunking &ch) {
-  return (ch.stuck || ch.loop == 1 || cta_for(ch.lim_last) == 128) ? 1 : 2;
-}
+// kernels launched by one sweep_* call: every sweep runs a last chunk of
+// more than 64 cells in the full chunks' launch, a shorter one in a launch
+// of its own
+int sweep_launches(const Chunking &ch) { return (ch.stuck || ch.loop == 1 || ch.lim_last > 64) ? 1 : 2; }
 
 // Per-device kernel attributes, set with the device current before the first
-// launch (pg_create): the packed polar kernels take their shared blocks as
-// dynamic shared memory, above the 48 KiB default limit for the 8-pencil
-// form, and prefer the largest shared-memory carveout so that 3 CTAs of it
-// (201 KB) fit on an SM.
+// launch (pg_create): the packed polar kernels and the column-packed radial
+// kernels take their shared blocks as dynamic shared memory, above the
+// 48 KiB default limit.
 int setup_device() {
   // 8 polar pencils of up to 44 cells: 52 KB of shared blocks per CTA.  No
   // carveout preference: the driver's choice leaves L1 room for the spill

@@ -131,8 +131,6 @@ void sweep_x(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c
 void sweep_y(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s);
 void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s);
 int sweep_launches(const Chunking &ch);
-int sweep_y_launches(const Chunking &ch);
-int sweep_x_launches(const Chunking &ch);
 // per-device kernel attributes (dynamic shared memory limits); 0 on success
 int setup_device();
 void cfl_full(const Tables &T, const double *r, const double *u, const double *v, const double *w,

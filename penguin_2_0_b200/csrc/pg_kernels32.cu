@@ -668,15 +668,19 @@ static inline int cta_for32(int lim) { return lim <= 32 ? 32 : (lim <= 64 ? 64 :
     else k32_sweep_y<SPHV, TD, 32, 1><<<grid, 32, 0, s>>>(T, P, ph, c, l0);                      \
   } while (0)
 
+// A last chunk of more than 64 cells runs in the full chunks' launch (the
+// bodies give chunk loop-1 its lim_last), as in the FP64 sweeps.
 void sweep_x32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
   const Chunking &ch = T.cx;
   int full = ch.stuck ? ch.loop : ch.loop - 1;
+  const bool merge = !ch.stuck && full > 0 && ch.lim_last > 64;
+  if (merge) full = ch.loop;
   if (full > 0) {
     dim3 grid(T.nphi, full, T.nk);
     if (ndim == 3) PG32_X(true, true, 128, grid, 0);
     else PG32_X(false, false, 128, grid, 0);
   }
-  if (!ch.stuck) {
+  if (!ch.stuck && !merge) {
     if (T.zpack && ch.lim_last <= PX32_LIM) {
       int npen = T.nphi * T.nk, blocks = (npen + 3) / 4, nt = 4 * ch.lim_last;
       if (ndim == 3) k32_sweep_x_packed<true, true, 4><<<blocks, nt, 0, s>>>(T, P, ph, c);
@@ -693,12 +697,14 @@ void sweep_x32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCt
 void sweep_y32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCtl &c, int ndim, cudaStream_t s) {
   const Chunking &ch = T.cy;
   int full = ch.stuck ? ch.loop : ch.loop - 1;
+  const bool merge = !ch.stuck && full > 0 && ch.lim_last > 64;
+  if (merge) full = ch.loop;
   if (full > 0) {
     dim3 grid(full, T.nr, T.nk);
     if (ndim == 3) PG32_Y(true, true, 128, grid, 0);
     else PG32_Y(false, false, 128, grid, 0);
   }
-  if (!ch.stuck) {
+  if (!ch.stuck && !merge) {
     dim3 grid(1, T.nr, T.nk);
     int nt = cta_for32(ch.lim_last), l0 = ch.loop - 1;
     if (ndim == 3) PG32_Y(true, true, nt, grid, l0);
@@ -714,11 +720,13 @@ void sweep_z32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCt
     return;
   }
   int full = ch.stuck ? ch.loop : ch.loop - 1;
+  const bool merge = !ch.stuck && full > 0 && ch.lim_last > 64;
+  if (merge) full = ch.loop;
   if (full > 0) {
     dim3 grid(T.nr, T.nphi, full);
     k32_sweep_z<128, 4><<<grid, 128, 0, s>>>(T, P, ph, c, ntop, 0);
   }
-  if (!ch.stuck) {
+  if (!ch.stuck && !merge) {
     dim3 grid(T.nr, T.nphi, 1);
     int nt = cta_for32(ch.lim_last), l0 = ch.loop - 1;
     if (nt == 32) k32_sweep_z<32, 1><<<grid, 32, 0, s>>>(T, P, ph, c, ntop, l0);

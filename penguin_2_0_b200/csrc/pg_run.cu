@@ -574,12 +574,8 @@ static pgd::SweepCtl host_ctl(double dt, const pg_body *pl, double frrot) {
   return c;
 }
 
-static int nx(pg_run *run) {
-  return run->fp32 ? pgk::sweep_launches(run->T.cx) : pgk::sweep_x_launches(run->T.cx);
-}
-static int ny(pg_run *run) {
-  return run->fp32 ? pgk::sweep_launches(run->T.cy) : pgk::sweep_y_launches(run->T.cy);
-}
+static int nx(pg_run *run) { return pgk::sweep_launches(run->T.cx); }
+static int ny(pg_run *run) { return pgk::sweep_launches(run->T.cy); }
 static int nz(pg_run *run) { return pgk::sweep_launches(run->T.cz); }
 
 // On a 3D run this is what the reference's bundle_sweep2D does on a 3D

@@ -45,10 +45,11 @@ struct ChunkShm32Data {
   double Rd[NT + 2], dld[NT + 2];   // FP64 Lagrangian density and face displacements
   double cf0;   // cos(phi - phi_planet) at the start of the step (radial, polar pencils)
 };
-// padded to 32 mod 128 bytes: conflict-free banks for 4 packed pencils
-template <int NT>
+// padded to TO mod 128 bytes: conflict-free banks for 128 / TO packed
+// pencils (32: four, 64: two)
+template <int NT, int TO = 32>
 struct ChunkShm32 : ChunkShm32Data<NT> {
-  char pad_[shm_pad_bytes((int)sizeof(ChunkShm32Data<NT>))];
+  char pad_[shm_pad_to((int)sizeof(ChunkShm32Data<NT>), TO)];
 };
 
 struct CellIn32 {
@@ -280,7 +281,7 @@ __device__ __forceinline__ double centre_force32(int n, double dt, double rad, d
 // azimuthal: w = v_r and in 3D v = v_theta, polar: v = v_r).  xa0 holds the
 // FP64 face coordinates.
 template <int AXIS, bool SPH, bool THREED, int NT>
-__device__ __forceinline__ double ppm_chunk32(ChunkShm32<NT> &S, int n, int nmax, double dt, double FrRot,
+__device__ __forceinline__ double ppm_chunk32(ChunkShm32Data<NT> &S, int n, int nmax, double dt, double FrRot,
                                             const CellIn32 &c, const Body &pl, const Phys &ph) {
   const bool act = n < nmax;
   const bool hasL = (AXIS != 1);

@@ -82,7 +82,7 @@ __device__ __forceinline__ void derivs_w(T &first, T &second, int n, const Deriv
 // One radial pencil chunk: column j0, chunk l, polar layer k.  The body is
 // shared by the per-run kernel and the batched kernels of pg_batch.cu.
 template <bool SPH, bool THREED, int NT>
-__device__ __forceinline__ void sweep_x32_body(ChunkShm32<NT> &S, int n, bool store, const Tables &T,
+__device__ __forceinline__ void sweep_x32_body(ChunkShm32Data<NT> &S, int n, bool store, const Tables &T,
                                                const Planes32 &P, const Phys &ph, const SweepCtl &ctl,
                                                const StepIn32 &st, int j0, int l, int k) {
   const bool last = (l == T.cx.loop - 1);
@@ -185,6 +185,28 @@ __global__ void __launch_bounds__(NT, MINB) k32_sweep_x(Tables T, Planes32 P, Ph
   if (!load_step32(ctl, st)) return;
   sweep_x32_body<SPH, THREED, NT>(S, threadIdx.x, true, T, P, ph, ctl, st, blockIdx.x, blockIdx.y + l0,
                                   blockIdx.z);
+}
+
+// Full radial chunks (and a last chunk of more than 64 cells, in the same
+// launch) of PACK adjacent columns per CTA, thread t on cell t / PACK of
+// column t % PACK, as k_sweep_x_cols: a warp's loads and stores of one ring
+// cover PACK adjacent floats.  The pencils' shared blocks are padded to
+// 128 / PACK mod 128 bytes.
+template <int PACK>
+using Px32Shm = ChunkShm32<ARR, 128 / PACK>;
+template <int PACK>
+constexpr int px32_shm_bytes() { return PACK * (int)sizeof(Px32Shm<PACK>); }
+template <bool SPH, bool THREED, int PACK, int MINB>
+__global__ void __launch_bounds__(ARR * PACK, MINB) k32_sweep_x_cols(Tables T, Planes32 P, Phys ph, SweepCtl ctl) {
+  extern __shared__ __align__(16) unsigned char px32_shm[];
+  Px32Shm<PACK> *S = reinterpret_cast<Px32Shm<PACK> *>(px32_shm);
+  StepIn32 st;
+  if (!load_step32(ctl, st)) return;
+  const int p = threadIdx.x % PACK, n = threadIdx.x / PACK;
+  int col = blockIdx.x * PACK + p;
+  const bool store = col < T.nphi;
+  if (!store) col = T.nphi - 1;
+  sweep_x32_body<SPH, THREED, ARR>(S[p], n, store, T, P, ph, ctl, st, col, blockIdx.y, blockIdx.z);
 }
 
 // short last chunks of radial pencils packed 4 columns per CTA (see
@@ -676,9 +698,17 @@ void sweep_x32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCt
   const bool merge = !ch.stuck && full > 0 && ch.lim_last > 64;
   if (merge) full = ch.loop;
   if (full > 0) {
-    dim3 grid(T.nphi, full, T.nk);
-    if (ndim == 3) PG32_X(true, true, 128, grid, 0);
-    else PG32_X(false, false, 128, grid, 0);
+    if (!ch.stuck && T.xpack == 2) {
+      // two adjacent columns per 256-thread CTA (a stuck last chunk keeps
+      // the one-column kernel)
+      dim3 grid((T.nphi + 1) / 2, full, T.nk);
+      if (ndim == 3) k32_sweep_x_cols<true, true, 2, 3><<<grid, 2 * ARR, px32_shm_bytes<2>(), s>>>(T, P, ph, c);
+      else k32_sweep_x_cols<false, false, 2, 3><<<grid, 2 * ARR, px32_shm_bytes<2>(), s>>>(T, P, ph, c);
+    } else {
+      dim3 grid(T.nphi, full, T.nk);
+      if (ndim == 3) PG32_X(true, true, 128, grid, 0);
+      else PG32_X(false, false, 128, grid, 0);
+    }
   }
   if (!ch.stuck && !merge) {
     if (T.zpack && ch.lim_last <= PX32_LIM) {

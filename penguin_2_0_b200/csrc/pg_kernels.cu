@@ -1579,7 +1579,8 @@ int setup_device() {
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(cols4[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   }
-  return e == cudaSuccess ? 0 : 1;
+  if (e != cudaSuccess) return 1;
+  return setup_device32();
 }
 
 void cfl_full(const Tables &T, const double *r, const double *u, const double *v, const double *w,

@@ -133,6 +133,7 @@ void sweep_z(const Tables &T, const Planes &P, const Phys &ph, const SweepCtl &c
 int sweep_launches(const Chunking &ch);
 // per-device kernel attributes (dynamic shared memory limits); 0 on success
 int setup_device();
+int setup_device32();
 void cfl_full(const Tables &T, const double *r, const double *u, const double *v, const double *w,
               const double *p0, const Phys &ph, double frrot, int ndim, unsigned long long *out,
               cudaStream_t s);

@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(NT, MINB) k32_sweep_y(Tables T, Planes32 P, Ph
 // One polar pencil chunk (ring i, column j0, chunk l), cell n of it; with
 // `store` false the pencil is computed and not stored.
 template <int NT>
-__device__ __forceinline__ void sweep_z32_body(ChunkShm32<NT> &S, int n, bool store, const Tables &T,
+__device__ __forceinline__ void sweep_z32_body(ChunkShm32Data<NT> &S, int n, bool store, const Tables &T,
                                                const Planes32 &P, const Phys &ph, const SweepCtl &ctl,
                                                const StepIn32 &st, int ntop, int i, int j0, int l) {
   const int nphi = T.nphi, nrg = T.nrg, nk = T.nk;
@@ -526,6 +526,28 @@ __global__ void __launch_bounds__(PACK * PZ32_LIM, MINB) k32_sweep_z_packed(Tabl
   const bool store = col < npen;
   if (!store) col = npen - 1;
   sweep_z32_body<PZ32_LIM>(S[p], n, store, T, P, ph, ctl, st, ntop, col / T.nphi, col % T.nphi, 0);
+}
+
+// Pencils of at most 44 cells (kmax 32) eight per CTA, as the FP64 packed
+// polar kernel: 352 threads = 11 whole warps (four pencils of 44 cells fill
+// 5.5 warps of a 6-warp CTA), 3 CTAs per SM, shared blocks sized for 44
+// cells and padded to 16 mod 128 bytes (dynamic: 8 of them take 50 KB).
+constexpr int PZ32_8_THREADS = 352;
+constexpr int PZ32_8_LIM = PZ32_8_THREADS / 8;
+using Pz32Shm8 = ChunkShm32<PZ32_8_LIM, 16>;
+constexpr int pz32_shm8_bytes() { return 8 * (int)sizeof(Pz32Shm8); }
+__global__ void __launch_bounds__(PZ32_8_THREADS, 3) k32_sweep_z_packed8(Tables T, Planes32 P, Phys ph, SweepCtl ctl,
+                                                                         int ntop) {
+  extern __shared__ __align__(16) unsigned char pz32_shm[];
+  Pz32Shm8 *S = reinterpret_cast<Pz32Shm8 *>(pz32_shm);
+  StepIn32 st;
+  if (!load_step32(ctl, st)) return;
+  const int p = threadIdx.x % 8, n = threadIdx.x / 8;
+  const int npen = T.nr * T.nphi;
+  int col = blockIdx.x * 8 + p;
+  const bool store = col < npen;
+  if (!store) col = npen - 1;
+  sweep_z32_body<PZ32_8_LIM>(S[p], n, store, T, P, ph, ctl, st, ntop, col / T.nphi, col % T.nphi, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -742,11 +764,20 @@ void sweep_y32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCt
   }
 }
 
+// the 8-pencil FP32 polar kernel's shared blocks exceed the 48 KiB default
+int setup_device32() {
+  return cudaFuncSetAttribute(k32_sweep_z_packed8, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              pz32_shm8_bytes()) == cudaSuccess ? 0 : 1;
+}
+
 void sweep_z32(const Tables &T, const Planes32 &P, const Phys &ph, const SweepCtl &c, int ntop, cudaStream_t s) {
   const Chunking &ch = T.cz;
   if (T.zpack && ch.loop == 1 && !ch.stuck && ch.lim_last <= PZ32_LIM) {
     int npen = T.nr * T.nphi;
-    k32_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
+    if (8 * ch.lim_last <= PZ32_8_THREADS)
+      k32_sweep_z_packed8<<<(npen + 7) / 8, 8 * ch.lim_last, pz32_shm8_bytes(), s>>>(T, P, ph, c, ntop);
+    else
+      k32_sweep_z_packed<4, 5><<<(npen + 3) / 4, 4 * ch.lim_last, 0, s>>>(T, P, ph, c, ntop);
     return;
   }
   int full = ch.stuck ? ch.loop : ch.loop - 1;

@@ -14,8 +14,9 @@ Tolerances, all relative to the FP64 run:
                     no planet and q <= 3e-5: L1(Sigma) <= 1e-4 (measured ~1e-6),
                     torque history <= 1e-3 of its max; q = 1e-3: see below
 Mass moves in FP64 inside the FP32 chain (displacements, widths, the density
-parabola and swept masses); that took q = 1e-4 on this disk from 1.9e-4 to
-6.0e-5 after 10 orbits.
+parabola and swept masses).  At q = 1e-4 this disk is 1.9e-4 off after 10
+orbits; most of that comes from the chain's FP32 arithmetic, not from the
+FP32 state planes (the same planes under an FP64 chain give 1.3e-5).
   3D, 40 steps      L1(rho) <= 1e-5
 """
 import numpy as np

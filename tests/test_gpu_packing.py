@@ -45,6 +45,10 @@ RADIAL_CASES = [
     dict(which=0, imax=252, jmax=390),                        # jmax not a multiple of 4: padding columns
     dict(which=1, imax=128, jmax=132, kmax=16),               # 3D
     dict(which=0, imax=232, jmax=200),                        # imax % 116 == 0: stuck last chunk
+    dict(which=0, imax=200, jmax=300),                        # last chunk 84 + 12 cells in the full chunks' launch
+    dict(which=0, imax=256, jmax=391, precision=1),           # FP32 (1 or 2 columns), an odd column count
+    dict(which=0, imax=200, jmax=300, precision=1),           # FP32, last chunk in the full chunks' launch
+    dict(which=1, imax=128, jmax=132, kmax=16, precision=1),  # FP32 3D
 ]
 
 
@@ -52,8 +56,8 @@ RADIAL_CASES = [
 @pytest.mark.parametrize("case", RADIAL_CASES)
 def test_radial_column_packing_is_bitwise(gpu, monkeypatch, case):
     """Full radial chunks run one column per CTA, or 2 or 4 adjacent columns
-    per CTA (PG_RADIAL_PACK): the same device body per cell, so the results
-    must be bitwise equal."""
+    per CTA (PG_RADIAL_PACK; FP32 runs take 1 or 2 and one column for 4):
+    the same device body per cell, so the results must be bitwise equal."""
     c = dict(case)
     p = pg.params(c.pop("which"), nprin=1, **c)
     ic = pg.build_ic(p)

@@ -936,6 +936,122 @@ __device__ __forceinline__ void reduce_body(const Tables &T, const RT *R, Body p
   }
 }
 
+// ---------------------------------------------------------------------------
+// Mass sums of runs with many rings: one warp per ring (RW rings per CTA).
+// Lane L holds list[L + 32 m], m = 0..31, of a 1024-cell block, its 32 loads
+// issued together; tree1024's levels 512..32 pair values inside a lane and
+// levels 16..1 across lanes by shuffle.  Every addition has the same two
+// operands as in tree1024, and __dadd_rn keeps the cell's product from being
+// fused into the first one, so the sums are bitwise those of reduce_body.
+// Used where cells are cheap (mass) and rings plentiful; the force sums and
+// small runs keep reduce_body's one cell per thread.
+constexpr int RW = 4;
+__device__ __forceinline__ double warp_tree1024(double (&v)[32]) {
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1) {
+#pragma unroll
+    for (int m = 0; m < h; m++) v[m] = __dadd_rn(v[m], v[m + h]);
+  }
+  double x = v[0];
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) {
+    const double y = __shfl_down_sync(0xffffffffu, x, d);
+    if (lane < d) x = __dadd_rn(x, y);
+  }
+  return x;   // lane 0: the block's sum
+}
+
+template <typename RT>
+__global__ void __launch_bounds__(32 * RW) k_reduce_mass_w(Tables T, const RT *R, const DevClock *clk, int ndim,
+                                                           double *ring_part, unsigned int *counter, double *out) {
+  __shared__ double list[1024];
+  __shared__ bool is_last;
+  if (clk && !clk->prin) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nr = T.nr, nk = T.nk, nphi = T.nphi;
+  for (int rt = blockIdx.x * RW + w; rt < nr * nk; rt += gridDim.x * RW) {
+    const int i = rt % nr, k = rt / nr;
+    const int row = i + NPAD, rk = k * T.nrg + row;
+    const size_t base = (size_t)rk * nphi;
+    const int rot = T.rot_j[rk];
+    const double xvol = T.rxvol[row];
+    const double zvol = (ndim == 3) ? T.zvol[k + NPAD] : 1.0;
+    // FP32 planes hold Sigma - S_bg(ring)
+    const double r_off = (sizeof(RT) == 4) ? T.sbg[rk] : 0.0;
+    const int loop = nphi / 1024 + (nphi % 1024 != 0);
+    double val = 0.0;
+    for (int l = 0; l < loop; l++) {
+      double v[32];
+#pragma unroll
+      for (int m = 0; m < 32; m++) {
+        const int j = lane + 32 * m + 1024 * l;   // storage index
+        double x = 0.0;
+        if (j < nphi) {
+          const int j0 = wrap1(j + rot, nphi);
+          const double r = r_off + (double)R[base + j0];
+          x = r * xvol * T.yvol[j0] * zvol;
+        }
+        v[m] = x;
+      }
+      const double sum = warp_tree1024(v);
+      if (lane == 0) val += sum;
+    }
+    if (lane == 0) ring_part[i + nr * k] = val;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned int prev = atomicAdd(counter, 1u);
+    is_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  // lv2 (3D: round_reduc_sum over k per ring, reduction.cu:77-100), then lv3
+  // over the rings in blocks of 1024, as reduce_body
+  const volatile double *part = ring_part;
+  double total = 0.0;
+  for (int base_i = 0; base_i < nr; base_i += 1024) {
+    for (int q4 = threadIdx.x; q4 < 1024; q4 += 32 * RW) {
+      const int ii = base_i + q4;
+      double v = 0.0;
+      if (ii < nr) {
+        if (ndim == 3) {
+          double acc[64];
+          int kk = nk < 64 ? nk : 64;
+          for (int q = 0; q < kk; q++) acc[q] = part[ii + nr * q];
+          int len2 = 1;
+          while (len2 < nk) len2 *= 2;
+          while (len2 > 1) {
+            int half = len2 / 2;
+            for (int q = 0; q < half; q++) if (q + half < kk) acc[q] += acc[q + half];
+            len2 = half;
+          }
+          v = acc[0];
+        } else {
+          v = part[ii];
+        }
+      }
+      list[q4] = v;
+    }
+    __syncthreads();
+    if (w == 0) {
+      double v[32];
+#pragma unroll
+      for (int m = 0; m < 32; m++) v[m] = list[lane + 32 * m];
+      const double sum = warp_tree1024(v);
+      if (lane == 0) total += sum;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double res = 0.0 + total;
+    if (out) *out = res;
+    *counter = 0u;
+  }
+}
+
 template <typename RT>
 __global__ void __launch_bounds__(1024) k_reduce(Tables T, const RT *R, Body pl, const DevClock *clk,
                                                  double exclude, int mode, int plnt, double p_alpha,
@@ -1632,9 +1748,19 @@ static int reduce_grid(const Tables &T) {
   return rings < 2 * nsm ? rings : 2 * nsm;
 }
 
+// The mass sums of a run with at least 1024 rings go one warp per ring
+// (k_reduce_mass_w): on the 128x1024x32 disk 4096 rings in one wave of
+// warps instead of 14 rings in turn per 1024-thread CTA.
+static bool mass_warp(const Tables &T) { return T.nr * T.nk >= 1024; }
+static int mass_grid(const Tables &T) { return (T.nr * T.nk + RW - 1) / RW; }
+
 void reduce(const Tables &T, const double *r, const Body &pl, const DevClock *clk, double exclude,
             int mode, int plnt, double p_alpha, int ndim, double *ring_part, unsigned int *counter,
             double *out, double *hist_row, cudaStream_t s) {
+  if ((mode == 0 || !plnt) && mass_warp(T)) {
+    k_reduce_mass_w<double><<<mass_grid(T), 32 * RW, 0, s>>>(T, r, clk, ndim, ring_part, counter, out);
+    return;
+  }
   k_reduce<double><<<reduce_grid(T), 1024, 0, s>>>(T, r, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter,
                                          out, hist_row);
 }
@@ -1642,6 +1768,10 @@ void reduce(const Tables &T, const double *r, const Body &pl, const DevClock *cl
 void reduce32(const Tables &T, const float *r, const Body &pl, const DevClock *clk, double exclude, int mode,
               int plnt, double p_alpha, int ndim, double *ring_part, unsigned int *counter, double *out,
               cudaStream_t s) {
+  if ((mode == 0 || !plnt) && mass_warp(T)) {
+    k_reduce_mass_w<float><<<mass_grid(T), 32 * RW, 0, s>>>(T, r, clk, ndim, ring_part, counter, out);
+    return;
+  }
   k_reduce<float><<<reduce_grid(T), 1024, 0, s>>>(T, r, pl, clk, exclude, mode, plnt, p_alpha, ndim, ring_part, counter,
                                         out, nullptr);
 }
